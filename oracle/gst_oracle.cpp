@@ -1,0 +1,784 @@
+// ORACLE -- test infrastructure only.
+//
+// CPU restatement of the reference's group Steiner tree (GST) solvers, used
+// by tests/, __graft_entry__.smoke() and the cpu_baseline leg of bench.py as
+// the checker.  Nothing in the engine links, calls or ships this file.
+//
+// Parity of this restatement is pinned against the reference programs
+// themselves: oracle/Makefile builds PrunedDP++ and D-PrunedDP++ from the
+// reference sources into oracle/_ref/, and tests/golden/make_golden.py runs
+// them on seeded inputs to produce the committed fixtures under tests/golden/.
+//
+// Entry points (C ABI, plain pointers):
+//   oracle_prunedpp   -- PrunedDP++ best-first search with its lower bounds and
+//                        pruning rules (code/PrunedDP++/include/CPUNONHOP.h:499-967)
+//   oracle_hop        -- diameter-bounded Dijkstra over (v, S, d)
+//                        (code/D-PrunedDP++/include/CPUHOP.h:107-288)
+//   oracle_dpbf       -- unpruned exact DPBF (Dijkstra over (v, S)); ground
+//                        truth used to check that the pruned solvers are exact
+//   oracle_validate   -- solution check: edges exist with their weights, the
+//                        edge set is a tree, it touches every queried group,
+//                        its weight equals the cost and its hop diameter <= D
+//                        (the reference only checks connectivity and cover:
+//                        this_is_a_feasible_solution_gpu,
+//                        code/PrunedDP++/include/exp_CPU_nonHop.h:17-49)
+//
+// Conventions shared with the reference:
+//   * inputs: undirected graph as CSR (both directions present), rows sorted
+//     by neighbour id; groups as CSR of member vertices; a query is a list of
+//     group ids (duplicates are merged, as the reference's unordered_set does);
+//   * bit i of a group set is the i-th distinct queried group;
+//   * the reference's "infinity" is 100000 (CPUNONHOP.h:14, CPUHOP.h:22); an
+//     infeasible query reports cost 100000 (exp_CPU_nonHop.h:120-126,
+//     exp_CPU_Hop.h:149-155).
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <queue>
+#include <set>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+
+namespace {
+
+constexpr int kInf = 100000;  // CPUNONHOP.h:14
+constexpr int kSafeguard = 2;  // error_safeguard, CPUNONHOP.h:512
+
+struct Csr {
+  int64_t V;
+  const int64_t* rowptr;
+  const int32_t* col;
+  const int32_t* w;
+};
+
+struct Groups {
+  const int64_t* ptr;
+  const int32_t* mem;
+  int64_t n;
+};
+
+// Weight of edge (a, b); rows are sorted by neighbour id.  -1 if absent.
+int edge_weight(const Csr& g, int a, int b) {
+  const int32_t* lo = g.col + g.rowptr[a];
+  const int32_t* hi = g.col + g.rowptr[a + 1];
+  const int32_t* it = std::lower_bound(lo, hi, b);
+  if (it == hi || *it != b) return -1;
+  return g.w[it - g.col];
+}
+
+// Distinct queried groups in first-seen order.
+std::vector<int> distinct_groups(const int32_t* q, int k) {
+  std::vector<int> out;
+  for (int i = 0; i < k; ++i)
+    if (std::find(out.begin(), out.end(), q[i]) == out.end()) out.push_back(q[i]);
+  return out;
+}
+
+// groupset(v) over the query's bits
+std::vector<int> vertex_groupsets(const Csr& g, const Groups& gr, const std::vector<int>& qg) {
+  std::vector<int> gs(g.V, 0);
+  for (size_t b = 0; b < qg.size(); ++b) {
+    int id = qg[b];
+    if (id < 0 || id >= gr.n) continue;
+    for (int64_t j = gr.ptr[id]; j < gr.ptr[id + 1]; ++j) gs[gr.mem[j]] |= 1 << b;
+  }
+  return gs;
+}
+
+// Multi-source Dijkstra from all members of a group with 0 start distance:
+// the dummy-vertex shortest paths of graph_v_of_v_idealID_PrunedDPPlusPlus_find_SPs_to_g
+// (CPUNONHOP.h:21-67).  Unreachable vertices keep kInf; pred[v] == v at sources.
+void group_sssp(const Csr& g, const Groups& gr, int gid, std::vector<int>& dist,
+                std::vector<int>& pred) {
+  dist.assign(g.V, kInf);
+  pred.resize(g.V);
+  for (int64_t v = 0; v < g.V; ++v) pred[v] = (int)v;
+  using E = std::pair<int, int>;
+  std::priority_queue<E, std::vector<E>, std::greater<E>> pq;
+  std::vector<char> done(g.V, 0);
+  std::vector<int> key(g.V, INT32_MAX);
+  if (gid >= 0 && gid < gr.n)
+    for (int64_t j = gr.ptr[gid]; j < gr.ptr[gid + 1]; ++j) {
+      int v = gr.mem[j];
+      key[v] = 0;
+      pq.push({0, v});
+    }
+  while (!pq.empty()) {
+    auto [d, v] = pq.top();
+    pq.pop();
+    if (done[v] || d != key[v]) continue;
+    done[v] = 1;
+    dist[v] = d;
+    for (int64_t j = g.rowptr[v]; j < g.rowptr[v + 1]; ++j) {
+      int u = g.col[j];
+      int nd = d + g.w[j];
+      if (!done[u] && nd < key[u]) {
+        key[u] = nd;
+        pred[u] = v;
+        pq.push({nd, u});
+      }
+    }
+  }
+}
+
+// Edge set of a solution as a sorted list of (min, max) pairs; duplicates are
+// merged the way graph_hash_of_mixed_weighted_add_edge merges them.
+struct EdgeSet {
+  std::set<std::pair<int, int>> e;
+  std::set<int> v;
+  void add_vertex(int a) { v.insert(a); }
+  void add_edge(int a, int b) {
+    v.insert(a);
+    v.insert(b);
+    e.insert({std::min(a, b), std::max(a, b)});
+  }
+  long long weight(const Csr& g) const {
+    long long s = 0;
+    for (auto& p : e) s += edge_weight(g, p.first, p.second);
+    return s;
+  }
+};
+
+struct UnionFind {
+  std::unordered_map<int, int> p;
+  int find(int x) {
+    auto it = p.find(x);
+    if (it == p.end()) {
+      p[x] = x;
+      return x;
+    }
+    if (it->second == x) return x;
+    int r = find(it->second);
+    p[x] = r;
+    return r;
+  }
+  bool unite(int a, int b) {
+    a = find(a);
+    b = find(b);
+    if (a == b) return false;
+    p[a] = b;
+    return true;
+  }
+};
+
+// Minimum spanning forest weight of the solution's own edges:
+// graph_hash_of_mixed_weighted_MST_postprocessing_no_whole_graph
+// (code/PrunedDP++/include/graph_hash_of_mixed_weighted_MST_postprocessing.h:10-35)
+long long mst_weight(const Csr& g, const EdgeSet& s) {
+  std::vector<std::pair<int, std::pair<int, int>>> es;
+  for (auto& p : s.e) es.push_back({edge_weight(g, p.first, p.second), p});
+  std::sort(es.begin(), es.end());
+  UnionFind uf;
+  long long tot = 0;
+  for (auto& x : es)
+    if (uf.unite(x.second.first, x.second.second)) tot += x.first;
+  return tot;
+}
+
+// Indexed binary min-heap over integer keys (state ids) with decrease-key.
+class StateHeap {
+ public:
+  explicit StateHeap(size_t n) : pos_(n, -1), pri_(n, 0) {}
+  bool contains(size_t id) const { return pos_[id] >= 0; }
+  int priority(size_t id) const { return pri_[id]; }
+  size_t size() const { return h_.size(); }
+  void push_or_decrease(size_t id, int p) {
+    if (pos_[id] < 0) {
+      pri_[id] = p;
+      pos_[id] = (long long)h_.size();
+      h_.push_back(id);
+      up(h_.size() - 1);
+    } else if (p < pri_[id]) {
+      pri_[id] = p;
+      up((size_t)pos_[id]);
+    }
+  }
+  size_t pop(int* p) {
+    size_t id = h_[0];
+    *p = pri_[id];
+    size_t last = h_.back();
+    h_.pop_back();
+    pos_[id] = -1;
+    if (!h_.empty() && last != id) {
+      h_[0] = last;
+      pos_[last] = 0;
+      down(0);
+    }
+    return id;
+  }
+
+ private:
+  bool less(size_t a, size_t b) const {
+    return pri_[h_[a]] < pri_[h_[b]] || (pri_[h_[a]] == pri_[h_[b]] && h_[a] < h_[b]);
+  }
+  void sw(size_t a, size_t b) {
+    std::swap(h_[a], h_[b]);
+    pos_[h_[a]] = (long long)a;
+    pos_[h_[b]] = (long long)b;
+  }
+  void up(size_t i) {
+    while (i > 0) {
+      size_t p = (i - 1) / 2;
+      if (less(i, p)) {
+        sw(i, p);
+        i = p;
+      } else break;
+    }
+  }
+  void down(size_t i) {
+    for (;;) {
+      size_t l = 2 * i + 1, r = l + 1, m = i;
+      if (l < h_.size() && less(l, m)) m = l;
+      if (r < h_.size() && less(r, m)) m = r;
+      if (m == i) break;
+      sw(i, m);
+      i = m;
+    }
+  }
+  std::vector<long long> pos_;
+  std::vector<int> pri_;
+  std::vector<size_t> h_;
+};
+
+struct TreeNode {  // graph_v_of_v_idealID_PrunedDPPlusPlus_tree_node, CPUNONHOP.h:99-111
+  int type = -1;   // 0 single vertex, 1 grow, 2 merge, -1 absent
+  int cost = kInf;
+  int u = -1;
+  int p1 = 0, p2 = 0;
+};
+
+void write_edges(const EdgeSet& s, const Csr& g, int32_t* edges, int cap, int* n_edges) {
+  int n = 0;
+  for (auto& p : s.e) {
+    if (n < cap && edges) {
+      edges[3 * n + 0] = p.first;
+      edges[3 * n + 1] = p.second;
+      edges[3 * n + 2] = edge_weight(g, p.first, p.second);
+    }
+    ++n;
+  }
+  if (n_edges) *n_edges = n;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Result of one oracle solve.
+typedef struct {
+  long long cost;        // reference-reported cost (100000 when infeasible)
+  int feasible;          // 1 if a tree touching every group was found
+  int root;              // root vertex of the returned tree (-1 if none)
+  int n_edges;           // edges written (may exceed cap: then truncated)
+  long long pops;        // states popped from the priority queue
+} oracle_result;
+
+// PrunedDP++ (Li et al., SIGMOD'16) as implemented by the reference,
+// graph_v_of_v_idealID_PrunedDPPlusPlus (code/PrunedDP++/include/CPUNONHOP.h:499-967).
+// Returns 0 on success, -1 on bad input.
+int oracle_prunedpp(int64_t V, const int64_t* rowptr, const int32_t* col, const int32_t* w,
+                    const int64_t* gptr, const int32_t* gmem, int64_t ngroups,
+                    const int32_t* query, int k_in, int32_t* edges, int edge_cap,
+                    oracle_result* out) {
+  if (!out || V <= 0 || k_in <= 0) return -1;
+  Csr g{V, rowptr, col, w};
+  Groups gr{gptr, gmem, ngroups};
+  std::vector<int> qg = distinct_groups(query, k_in);
+  const int k = (int)qg.size();
+  if (k >= 15) return -1;  // CPUNONHOP.h:505-509
+  const int full = (1 << k) - 1;
+  const int W = 1 << k;
+  out->pops = 0;
+
+  // find_SPs: CPUNONHOP.h:21-80
+  std::vector<std::vector<int>> dist(k), pred(k);
+  for (int i = 0; i < k; ++i) group_sssp(g, gr, qg[i], dist[i], pred[i]);
+
+  // virtual_node_distances: CPUNONHOP.h:175-210 (min over members of the
+  // second group of the first group's distances)
+  std::vector<std::vector<int>> vnd(k, std::vector<int>(k, kInf));
+  for (int a = 0; a < k; ++a)
+    for (int b = a; b < k; ++b) {
+      int d = kInf;
+      if (qg[b] < ngroups)
+        for (int64_t j = gptr[qg[b]]; j < gptr[qg[b] + 1]; ++j) d = std::min(d, dist[a][gmem[j]]);
+      vnd[a][b] = vnd[b][a] = d;
+    }
+
+  // AllPaths: CPUNONHOP.h:269-386.  Wm[i][j][X] plays W["g_i"+"_"+"g_j"+"_"+X];
+  // lookups of absent keys read 0, as std::unordered_map::operator[] does.
+  const size_t WN = (size_t)k * k * W;
+  std::vector<int> Wm(WN, 0);
+  std::vector<char> Whas(WN, 0);
+  {
+    auto id = [&](int i, int j, int X) { return ((size_t)i * k + j) * W + X; };
+    StateHeap Q(WN);
+    std::vector<char> Dset(WN, 0);
+    for (int i = 0; i < k; ++i) Q.push_or_decrease(id(i, i, 0), 0);
+    while (Q.size() > 0) {
+      int cost;
+      size_t s = Q.pop(&cost);
+      int X = (int)(s % W), j = (int)((s / W) % k), i = (int)(s / W / k);
+      Wm[s] = cost;  // overwritten on pop, as CPUNONHOP.h:314
+      Whas[s] = 1;
+      Dset[s] = 1;
+      for (int sub = 0; sub < X; ++sub)
+        if ((sub | X) == X) {
+          size_t t = id(i, j, sub);
+          if (!Whas[t] || Wm[t] > cost) {
+            Wm[t] = cost;
+            Whas[t] = 1;
+          }
+        }
+      for (int p = 0; p < k; ++p) {
+        int pb = 1 << p;
+        if ((pb | X) != X) {
+          size_t t = id(i, p, X + pb);
+          if (Dset[t]) continue;
+          Q.push_or_decrease(t, cost + vnd[j][p]);
+        }
+      }
+    }
+  }
+  auto Wat = [&](int i, int j, int X) { return Wm[((size_t)i * k + j) * W + X]; };
+  // W2: CPUNONHOP.h:568-587
+  std::vector<int> W2((size_t)k * W, kInf);
+  for (int i = 0; i < k; ++i)
+    for (int X = 1; X <= full; ++X) {
+      int d = kInf;
+      for (int j = 0; j < k; ++j) d = std::min(d, Wat(i, j, X));
+      W2[(size_t)i * W + X] = d;
+    }
+
+  // LB_procedure: CPUNONHOP.h:436-496 (integer halving as in the reference)
+  auto lb_of = [&](int v, int X, int cost) -> int {
+    if (X == full) return cost;
+    int Xs = full - X;
+    int lb1 = kInf, lb2 = -1, one = -1;
+    for (int i = 0; i < k; ++i) {
+      if ((Xs >> i & 1) == 0) continue;
+      int di = dist[i][v];
+      int xxx = kInf;
+      for (int j = 0; j < k; ++j) {
+        if ((Xs >> j & 1) == 0) continue;
+        int dj = dist[j][v];
+        xxx = std::min(xxx, dj);
+        lb1 = std::min(lb1, (di + Wat(i, j, Xs) + dj) / 2);
+      }
+      lb2 = std::max(lb2, (di + W2[(size_t)i * W + Xs] + xxx) / 2);
+      one = std::max(one, di);
+    }
+    int lb = lb1 < lb2 ? lb2 : lb1;
+    if (lb < one) lb = one;
+    return cost + lb;
+  };
+
+  std::vector<int> gs = vertex_groupsets(g, gr, qg);
+  const size_t NS = (size_t)V * W;
+  std::vector<TreeNode> trees(NS);
+  std::vector<char> popped(NS, 0);
+  StateHeap QT(NS);
+  auto sid = [&](int v, int p) { return (size_t)v * W + p; };
+  // seed: CPUNONHOP.h:594-624
+  for (int v = 0; v < V; ++v)
+    for (int p = 1; p <= gs[v]; ++p)
+      if ((p | gs[v]) == gs[v]) {
+        trees[sid(v, p)].type = 0;
+        trees[sid(v, p)].cost = 0;
+        QT.push_or_decrease(sid(v, p), 0);
+      }
+
+  // build_tree: CPUNONHOP.h:390-432
+  auto build_tree = [&](int rv, int rp, EdgeSet& s) {
+    std::vector<std::pair<int, int>> st{{rv, rp}};
+    while (!st.empty()) {
+      auto [v, p] = st.back();
+      st.pop_back();
+      s.add_vertex(v);
+      const TreeNode& t = trees[sid(v, p)];
+      if (t.type == 1) {
+        st.push_back({t.u, p});
+        s.add_edge(t.u, v);
+      } else if (t.type == 2) {
+        st.push_back({v, t.p1});
+        st.push_back({v, t.p2});
+      }
+    }
+  };
+
+  std::vector<std::vector<int>> uncovered(W);
+  for (int p = 0; p <= full; ++p)
+    for (int i = 0; i < k; ++i)
+      if (!(p >> i & 1)) uncovered[p].push_back(i);
+
+  int best_cost = kInf;
+  EdgeSet answer;
+  out->feasible = 0;
+  out->root = -1;
+  while (QT.size() > 0) {
+    int prio;
+    size_t s = QT.pop(&prio);
+    out->pops++;
+    int v = (int)(s / W), X = (int)(s % W);
+    int vx = trees[s].cost;
+    if (X == full) {  // CPUNONHOP.h:658-678
+      build_tree(v, X, answer);
+      out->feasible = 1;
+      out->root = v;
+      break;
+    }
+    popped[s] = 1;
+    // one-label feasible solution: CPUNONHOP.h:684-726
+    int fcost = vx;
+    for (int i : uncovered[X]) {
+      if (dist[i][v] == kInf) {
+        fcost = kInf;
+        break;
+      }
+      fcost += dist[i][v];
+    }
+    if (fcost < best_cost) {
+      EdgeSet fs;
+      build_tree(v, X, fs);
+      for (int i : uncovered[X]) {
+        int a = v, p = pred[i][a];
+        while (a != p) {
+          fs.add_edge(a, p);
+          a = p;
+          p = pred[i][a];
+        }
+      }
+      best_cost = (int)mst_weight(g, fs);
+    }
+    // complement merge: CPUNONHOP.h:733-792
+    int Xs = full - X;
+    if (popped[sid(v, Xs)]) {
+      int merged = vx + trees[sid(v, Xs)].cost;
+      TreeNode& tf = trees[sid(v, full)];
+      if (merged < tf.cost) {
+        tf.type = 2;
+        tf.cost = merged;
+        tf.p1 = X;
+        tf.p2 = Xs;
+        if (merged > best_cost + kSafeguard) continue;
+        if (merged < best_cost) best_cost = merged;
+        QT.push_or_decrease(sid(v, full), merged);
+      }
+      continue;
+    }
+    // decomposition theorem: CPUNONHOP.h:795
+    if (vx < best_cost / 2 + kSafeguard) {
+      // grow: CPUNONHOP.h:801-869
+      for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j) {
+        int u = col[j];
+        size_t t = sid(u, X);
+        if (popped[t]) continue;
+        int gc = vx + w[j];
+        if (gc < trees[t].cost) {
+          trees[t].type = 1;
+          trees[t].cost = gc;
+          trees[t].u = v;
+          if (lb_of(u, X, gc) > best_cost + kSafeguard) continue;
+          QT.push_or_decrease(t, gc);
+        }
+      }
+      // merge: CPUNONHOP.h:874-958, partners j = 1..full-1 disjoint from X
+      for (int p2 = 1; p2 < full; ++p2) {
+        if (p2 & X) continue;
+        if (!popped[sid(v, p2)]) continue;
+        int pu = X + p2;
+        size_t t = sid(v, pu);
+        if (popped[t]) continue;
+        int mc = vx + trees[sid(v, p2)].cost;
+        if (mc < trees[t].cost) {
+          trees[t].type = 2;
+          trees[t].cost = mc;
+          trees[t].p1 = X;
+          trees[t].p2 = p2;
+          if (mc <= best_cost * 0.667 + kSafeguard) {
+            if (lb_of(v, pu, mc) > best_cost + kSafeguard) continue;
+            if (pu == full && mc < best_cost) best_cost = mc;
+            QT.push_or_decrease(t, mc);
+          }
+        }
+      }
+    }
+  }
+  if (out->feasible) {
+    out->cost = answer.weight(g);
+    write_edges(answer, g, edges, edge_cap, &out->n_edges);
+  } else {
+    out->cost = kInf;  // exp_CPU_nonHop.h:120-126
+    out->n_edges = 0;
+  }
+  return 0;
+}
+
+// Unpruned exact DPBF: Dijkstra over (v, S) with grow over every edge and merge
+// with every settled disjoint partner.  Optimal by construction; used to check
+// that the pruned solvers are exact.  Infeasible -> cost 100000.
+int oracle_dpbf(int64_t V, const int64_t* rowptr, const int32_t* col, const int32_t* w,
+                const int64_t* gptr, const int32_t* gmem, int64_t ngroups, const int32_t* query,
+                int k_in, int32_t* edges, int edge_cap, oracle_result* out) {
+  if (!out || V <= 0 || k_in <= 0) return -1;
+  Csr g{V, rowptr, col, w};
+  Groups gr{gptr, gmem, ngroups};
+  std::vector<int> qg = distinct_groups(query, k_in);
+  const int k = (int)qg.size();
+  if (k > 20) return -1;
+  const int full = (1 << k) - 1, W = 1 << k;
+  std::vector<int> gs = vertex_groupsets(g, gr, qg);
+  const size_t NS = (size_t)V * W;
+  std::vector<TreeNode> tr(NS);
+  std::vector<char> settled(NS, 0);
+  StateHeap Q(NS);
+  for (int v = 0; v < V; ++v)
+    for (int p = 1; p <= gs[v]; ++p)
+      if ((p | gs[v]) == gs[v]) {
+        tr[(size_t)v * W + p].type = 0;
+        tr[(size_t)v * W + p].cost = 0;
+        Q.push_or_decrease((size_t)v * W + p, 0);
+      }
+  out->pops = 0;
+  out->feasible = 0;
+  out->root = -1;
+  int root = -1;
+  while (Q.size() > 0) {
+    int c;
+    size_t s = Q.pop(&c);
+    out->pops++;
+    int v = (int)(s / W), X = (int)(s % W);
+    settled[s] = 1;
+    if (X == full) {
+      root = v;
+      break;
+    }
+    for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j) {
+      size_t t = (size_t)col[j] * W + X;
+      if (settled[t]) continue;
+      int nc = c + w[j];
+      if (nc < tr[t].cost) {
+        tr[t] = TreeNode{1, nc, v, 0, 0};
+        Q.push_or_decrease(t, nc);
+      }
+    }
+    int comp = full ^ X;
+    for (int p2 = comp; p2 > 0; p2 = (p2 - 1) & comp) {
+      size_t o = (size_t)v * W + p2;
+      if (!settled[o]) continue;
+      size_t t = (size_t)v * W + (X | p2);
+      if (settled[t]) continue;
+      int nc = c + tr[o].cost;
+      if (nc < tr[t].cost) {
+        tr[t] = TreeNode{2, nc, -1, X, p2};
+        Q.push_or_decrease(t, nc);
+      }
+    }
+  }
+  if (root < 0) {
+    out->cost = kInf;
+    out->n_edges = 0;
+    return 0;
+  }
+  EdgeSet s;
+  std::vector<std::pair<int, int>> st{{root, full}};
+  while (!st.empty()) {
+    auto [v, p] = st.back();
+    st.pop_back();
+    s.add_vertex(v);
+    const TreeNode& t = tr[(size_t)v * W + p];
+    if (t.type == 1) {
+      s.add_edge(t.u, v);
+      st.push_back({t.u, p});
+    } else if (t.type == 2) {
+      st.push_back({v, t.p1});
+      st.push_back({v, t.p2});
+    }
+  }
+  out->feasible = 1;
+  out->root = root;
+  out->cost = tr[(size_t)root * W + full].cost;
+  write_edges(s, g, edges, edge_cap, &out->n_edges);
+  return 0;
+}
+
+// HOP_cpu (code/D-PrunedDP++/include/CPUHOP.h:107-288): Dijkstra with lazy
+// deletion over (v, p, d); grow (v,p,d)->(u,p,d+1) when d < D; merge
+// (v,p1,d1)+(v,p2,d2) with p1 & p2 == 0 and d2 <= D - d1 into
+// (v, p1|p2, max(d1,d2)); stops at the first settled full set.  Reported cost
+// is the weight of the de-duplicated edge set (exp_CPU_Hop.h:146), 100000
+// when infeasible.
+int oracle_hop(int64_t V, const int64_t* rowptr, const int32_t* col, const int32_t* w,
+               const int64_t* gptr, const int32_t* gmem, int64_t ngroups, const int32_t* query,
+               int k_in, int D, int32_t* edges, int edge_cap, oracle_result* out) {
+  if (!out || V <= 0 || k_in <= 0 || D < 0) return -1;
+  Csr g{V, rowptr, col, w};
+  Groups gr{gptr, gmem, ngroups};
+  std::vector<int> qg = distinct_groups(query, k_in);
+  const int k = (int)qg.size();
+  if (k > 16) return -1;
+  const int full = (1 << k) - 1, W = 1 << k, DD = D + 1;
+  struct HNode {
+    int cost = kInf, type = -1, u = -1, p1 = 0, p2 = 0, d1 = 0, d2 = 0;
+  };
+  const size_t NS = (size_t)V * W * DD;
+  std::vector<HNode> t(NS);
+  auto id = [&](int v, int p, int d) { return ((size_t)v * W + p) * DD + d; };
+  std::vector<int> gs = vertex_groupsets(g, gr, qg);
+  struct QE {
+    int cost, v, p, d;
+    bool operator>(const QE& o) const { return cost > o.cost; }
+  };
+  std::priority_queue<QE, std::vector<QE>, std::greater<QE>> q;
+  // CPUHOP.h:157-170 seeds singleton sets only
+  for (int v = 0; v < V; ++v)
+    for (int i = 0; i < k; ++i)
+      if (gs[v] >> i & 1) {
+        HNode& n = t[id(v, 1 << i, 0)];
+        n.cost = 0;
+        n.type = 0;
+        q.push({0, v, 1 << i, 0});
+      }
+  out->pops = 0;
+  out->feasible = 0;
+  out->root = -1;
+  int rv = -1, rd = -1;
+  while (!q.empty()) {
+    QE e = q.top();
+    q.pop();
+    out->pops++;
+    if (e.cost != t[id(e.v, e.p, e.d)].cost) continue;
+    if (e.p == full) {
+      rv = e.v;
+      rd = e.d;
+      break;
+    }
+    if (e.d < D)
+      for (int64_t j = rowptr[e.v]; j < rowptr[e.v + 1]; ++j) {
+        int u = col[j];
+        HNode& n = t[id(u, e.p, e.d + 1)];
+        if (n.cost > e.cost + w[j]) {
+          n.cost = e.cost + w[j];
+          n.type = 1;
+          n.u = e.v;
+          q.push({n.cost, u, e.p, e.d + 1});
+        }
+      }
+    for (int p2 = 1; p2 <= full; ++p2) {
+      if (p2 & e.p) continue;
+      for (int d2 = 0; d2 <= D - e.d; ++d2) {
+        int pu = e.p | p2, nd = std::max(e.d, d2);
+        int mc = e.cost + t[id(e.v, p2, d2)].cost;
+        HNode& n = t[id(e.v, pu, nd)];
+        if (n.cost > mc) {
+          n.cost = mc;
+          n.type = 2;
+          n.p1 = e.p;
+          n.p2 = p2;
+          n.d1 = e.d;
+          n.d2 = d2;
+          q.push({mc, e.v, pu, nd});
+        }
+      }
+    }
+  }
+  if (rv < 0) {
+    out->cost = kInf;
+    out->n_edges = 0;
+    return 0;
+  }
+  EdgeSet s;
+  struct Item {
+    int v, p, d;
+  };
+  std::vector<Item> st{{rv, full, rd}};
+  while (!st.empty()) {
+    Item it = st.back();
+    st.pop_back();
+    s.add_vertex(it.v);
+    const HNode& n = t[id(it.v, it.p, it.d)];
+    if (n.type == 1) {
+      s.add_edge(n.u, it.v);
+      st.push_back({n.u, it.p, it.d - 1});
+    } else if (n.type == 2) {
+      st.push_back({it.v, n.p1, n.d1});
+      st.push_back({it.v, n.p2, n.d2});
+    }
+  }
+  out->feasible = 1;
+  out->root = rv;
+  out->cost = s.weight(g);
+  write_edges(s, g, edges, edge_cap, &out->n_edges);
+  return 0;
+}
+
+// Checks a solution.  Returns 0 if valid, else a positive code:
+//   1 an edge is not in the graph or has a different weight
+//   2 the edge set is not a tree (cycle or disconnected)
+//   3 a queried group is not touched
+//   4 the weight differs from `cost`
+//   5 the hop diameter exceeds D (D < 0: unbounded)
+// A single-vertex solution (n_edges == 0) is passed as `root`.
+int oracle_validate(int64_t V, const int64_t* rowptr, const int32_t* col, const int32_t* w,
+                    const int64_t* gptr, const int32_t* gmem, int64_t ngroups,
+                    const int32_t* query, int k, const int32_t* edges, int n_edges, int root,
+                    long long cost, int D) {
+  Csr g{V, rowptr, col, w};
+  std::unordered_map<int, std::vector<int>> adj;
+  long long tot = 0;
+  UnionFind uf;
+  for (int e = 0; e < n_edges; ++e) {
+    int a = edges[3 * e], b = edges[3 * e + 1], c = edges[3 * e + 2];
+    if (a < 0 || b < 0 || a >= V || b >= V) return 1;
+    if (edge_weight(g, a, b) != c) return 1;
+    if (!uf.unite(a, b)) return 2;
+    adj[a].push_back(b);
+    adj[b].push_back(a);
+    tot += c;
+  }
+  if (n_edges == 0) {
+    if (root < 0 || root >= V) return 2;
+    adj[root];
+  }
+  int r0 = adj.begin()->first;
+  for (auto& kv : adj)
+    if (uf.find(kv.first) != uf.find(r0)) return 2;
+  for (int i = 0; i < k; ++i) {
+    int gid = query[i];
+    bool hit = false;
+    if (gid >= 0 && gid < ngroups)
+      for (int64_t j = gptr[gid]; j < gptr[gid + 1] && !hit; ++j) hit = adj.count(gmem[j]) > 0;
+    if (!hit) return 3;
+  }
+  if (tot != cost) return 4;
+  if (D >= 0) {
+    auto bfs = [&](int s, int* far) {
+      std::unordered_map<int, int> dd{{s, 0}};
+      std::vector<int> fr{s};
+      int best = 0;
+      *far = s;
+      for (size_t i = 0; i < fr.size(); ++i) {
+        int x = fr[i];
+        for (int y : adj[x])
+          if (!dd.count(y)) {
+            dd[y] = dd[x] + 1;
+            if (dd[y] > best) {
+              best = dd[y];
+              *far = y;
+            }
+            fr.push_back(y);
+          }
+      }
+      return best;
+    };
+    int a, b;
+    bfs(r0, &a);
+    int diam = bfs(a, &b);
+    if (diam > D) return 5;
+  }
+  return 0;
+}
+
+}  // extern "C"
