@@ -1,0 +1,123 @@
+// Device-side data layout and helpers of the GST engine.
+//
+// One query occupies a "slot".  Its DP table lives in a slab of the device
+// arena:
+//
+//   table[v][idx(S)][l]   int32, row = W*L ints per vertex, W = 2^k, L = 1
+//                          (plain) or D+1 (diameter bound D).  idx orders the
+//                          2^k subsets by (popcount, value), so the sets of one
+//                          layer |S| = s are contiguous in a row; l is the
+//                          depth label of the D- variants, innermost so that
+//                          the labels of one (v, S) share a sector.
+//   mask[l][v]            uint64 dirty bits over the ranks of the current
+//                          layer's sets: (v, S, l) improved and must be grown.
+//   queue[qi][v]          frontier vertex lists (plain: 2 ping-pong lists;
+//                          D-: one list per depth label).
+//   touched[], tflag[v]   vertices that ever held a finite entry.
+//   chunks[]              the current round's grow work: (v, edge range, mask).
+//
+// INF = 0x3f3f3f3f so that a byte memset initialises a table and the sum of
+// two INF entries does not overflow int32.
+#pragma once
+#include <cstdint>
+
+#include "gst_b200.h"
+
+namespace gst {
+
+constexpr int INF = 0x3f3f3f3f;
+constexpr int MAXK = GST_MAX_K;
+constexpr int MAXW = 1 << MAXK;
+constexpr int MAXL = GST_MAX_D + 1;
+constexpr int MAXSLOTS = 1024;
+constexpr int MAXQ = MAXL + 1;  // queue lists per slot
+
+enum Phase : int32_t { PH_FREE = 0, PH_ACTIVE = 1, PH_DONE = 2, PH_ERROR = 3 };
+enum Action : int32_t {
+  A_NONE = 0,
+  A_INIT = 1,      // seeds written by the admission kernels
+  A_GROW = 2,      // prep + relax one frontier
+  A_LBPREP = 3,    // lower-bound tables after the singleton layer
+  A_MERGE = 4,     // subset join of the next layer
+  A_MERGEFULL = 5  // join of the full set: the answer
+};
+enum Err : int32_t {
+  ERR_NONE = 0,
+  ERR_CHUNK_CAP = 1,
+  ERR_QUEUE_CAP = 2,
+  ERR_WITNESS = 3,
+  ERR_WITNESS_CAP = 4,
+  ERR_ROUNDS = 5
+};
+
+struct Chunk {
+  uint32_t v;
+  uint32_t eb;  // first edge (absolute CSR index)
+  uint32_t ee;  // one past the last edge
+  uint32_t pad;
+  unsigned long long mask;  // dirty set ranks snapshotted by the prep pass
+};
+
+struct Slot {
+  // ---- set at admission --------------------------------------------------
+  int32_t* table;
+  unsigned long long* mask;
+  uint32_t* queue;
+  uint32_t* touched;
+  uint32_t* tflag;
+  Chunk* chunks;
+  int32_t* lbtab;   // P[k][k][W] then W2[k][W]
+  int32_t* wstack;  // witness search stack, 4 ints per entry
+  int32_t* wedges;  // witness output, 3 ints per edge
+  long long chunk_cap;
+  long long wcap;
+  int32_t k, W, L, D;  // D < 0: plain
+  int32_t groups[MAXK];
+  int32_t max_rounds;
+  // ---- dynamic -------------------------------------------------------------
+  int32_t phase, action;
+  int32_t s;    // current layer |S|
+  int32_t d;    // current depth label (D- variants)
+  int32_t cur;  // current ping-pong list (plain)
+  int32_t best; // upper bound: cost of a known feasible solution
+  int32_t R1;   // singleton distances above R1 are only known to exceed R1
+  int32_t err;
+  int32_t ntouched, nchunks, nwedges;
+  int32_t rounds;
+  int32_t qcount[MAXQ];
+  unsigned long long answer;  // (cost << 32) | root
+  unsigned long long st_frontier, st_relax, st_improve, st_merges;
+};
+
+struct SlotStatus {
+  int32_t phase;
+  int32_t err;
+  unsigned long long answer;
+};
+
+struct Plan {
+  int32_t n_lb, n_merge, n_grow, n_active;
+  int32_t lb_slots[MAXSLOTS];
+  int32_t merge_slots[MAXSLOTS];
+  int32_t grow_slots[MAXSLOTS];
+  long long merge_off[MAXSLOTS + 1];
+  long long prep_off[MAXSLOTS + 1];
+  long long chunk_off[MAXSLOTS + 1];
+};
+
+// Subset orderings for k = 1..MAXK (popcount, then value).
+struct SubsetTables {
+  uint8_t sidx[MAXK + 1][MAXW];     // S -> index
+  uint8_t sof[MAXK + 1][MAXW];      // index -> S
+  uint8_t loff[MAXK + 1][MAXK + 2]; // first index of layer s
+};
+
+struct Graph {
+  const long long* rowptr;  // V+1
+  const int2* adj;          // E x (neighbour, weight)
+  const long long* gptr;    // groups: n+1
+  const int32_t* gmem;
+  long long V, E, G;
+};
+
+}  // namespace gst

@@ -1,0 +1,761 @@
+// Round kernels of the GST engine (sm_100a).
+//
+// A query runs the DP layer by layer over |S| (the "layered DPBF"):
+//   layer 1   k singleton shortest-path trees grown from the group members
+//             (the one-label distances of dis0_init_1, code/TrimCDP/src/DPQ.cu:241-271);
+//   lbprep    group-to-group bounds and Held-Karp path table for the tour
+//             lower bounds (host W/W1 tables of code/TrimCDP/src/DPQ.cu:409-483,
+//             LB_procedure of code/PrunedDP++/include/CPUNONHOP.h:436-496);
+//   layer s   subset join at every touched vertex (merge,
+//             code/TrimCDP/src/DPQ.cu:140-170) followed by frontier edge
+//             relaxation until no state of the layer improves (grow, :112-137);
+//   layer k   join of the full set at every vertex: the answer.
+// The D- variants carry a depth label per state (code/D-TrimCDP/src/DPQ.cu:62-120):
+// grow moves label l to l+1 (l < D); merging labels l1, l2 needs l1 + l2 <= D and
+// yields max(l1, l2).  Tables hold the best cost found with that label; a value
+// is only stored when it beats every smaller label, so prefix minima over labels
+// are the costs "with depth at most l".
+//
+// Pruning (all admissible, so every optimal derivation survives):
+//   * grow sources must cost at most best/2 (optimal-tree decomposition,
+//     PrunedDP++ Theorem 1, CPUNONHOP.h:795);
+//   * a state is dropped when cost + lb(v, S) > best, lb the max of the
+//     one-label bound and the two tour bounds of LB_procedure (rounded up:
+//     the tree cost is an integer at least half the tour).
+// All kernels run on a fixed grid and read their work sizes from device
+// memory, so a round (ctl_a, lbprep, merge, prep, ctl_b, grow) can be captured
+// once in a CUDA graph and replayed.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "engine_dev.cuh"
+
+namespace gst {
+
+__constant__ SubsetTables c_sub;
+
+__device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
+__device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
+
+// Largest j in [0, n) with off[j] <= g (off[0] = 0, off[n] = total > g).
+__device__ __forceinline__ int seg_search(const long long* off, int n, long long g) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= g) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void touch(Slot& q, uint32_t u) {
+  if (q.tflag[u] == 0 && atomicExch(&q.tflag[u], 1u) == 0u) {
+    int p = atomicAdd(&q.ntouched, 1);
+    q.touched[p] = u;
+  }
+}
+
+// Marks (u, rank r, label l) dirty and enqueues u on the list qi if it was clean.
+__device__ __forceinline__ void mark_dirty(Slot& q, long long V, uint32_t u, int r, int mi, int qi) {
+  unsigned long long om = atomicOr(&q.mask[(long long)mi * V + u], 1ull << r);
+  if (om == 0ull) {
+    int pos = atomicAdd(&q.qcount[qi], 1);
+    if (pos < V) q.queue[(long long)qi * V + pos] = u;
+    else q.err = ERR_QUEUE_CAP;
+  }
+}
+
+// Distance lower bound of v to singleton group i: entries above R1 only tell
+// that the distance exceeds R1.
+__device__ __forceinline__ int clip_dist(int d, int R1) { return d > R1 ? R1 + 1 : d; }
+
+// Tour / one-label lower bound for completing (v, S) given the clipped
+// singleton distances dist[0..k) of v (LB_procedure, CPUNONHOP.h:436-496).
+__device__ __forceinline__ int lower_bound(const int* dist, int k, int W, int S,
+                                           const int32_t* lbtab) {
+  const int full = W - 1;
+  const int Xs = full ^ S;
+  if (Xs == 0) return 0;
+  int one = 0, mind = INF;
+  for (int i = 0; i < k; ++i)
+    if (Xs >> i & 1) {
+      one = imax(one, dist[i]);
+      mind = imin(mind, dist[i]);
+    }
+  long long lb1 = INF, lb2 = 0;
+  const int32_t* W2 = lbtab + (size_t)k * k * W;
+  for (int i = 0; i < k; ++i) {
+    if (!(Xs >> i & 1)) continue;
+    for (int j = 0; j < k; ++j) {
+      if (!(Xs >> j & 1)) continue;
+      long long t = (long long)dist[i] + lbtab[(i * k + j) * W + Xs] + dist[j];
+      t = (t + 1) >> 1;
+      if (t < lb1) lb1 = t;
+    }
+    long long t2 = (long long)dist[i] + W2[i * W + Xs] + mind;
+    t2 = (t2 + 1) >> 1;
+    if (t2 > lb2) lb2 = t2;
+  }
+  long long lb = one;
+  if (lb1 > lb && lb1 < INF) lb = lb1;
+  if (lb2 > lb) lb = lb2;
+  return (int)(lb < INF ? lb : INF);
+}
+
+// ---------------------------------------------------------------------------
+// Admission: seed the singleton states of the group members.
+// ---------------------------------------------------------------------------
+__global__ void k_init_seeds(Slot* slots, int t, Graph g) {
+  Slot& q = slots[t];
+  const int k = q.k, L = q.L, rowlen = q.W * q.L;
+  long long total = 0;
+  for (int i = 0; i < k; ++i) total += g.gptr[q.groups[i] + 1] - g.gptr[q.groups[i]];
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
+       x += (long long)gridDim.x * blockDim.x) {
+    long long rem = x;
+    int i = 0;
+    for (; i < k; ++i) {
+      long long n = g.gptr[q.groups[i] + 1] - g.gptr[q.groups[i]];
+      if (rem < n) break;
+      rem -= n;
+    }
+    uint32_t v = (uint32_t)g.gmem[g.gptr[q.groups[i]] + rem];
+    q.table[(long long)v * rowlen + (1 + i) * L + 0] = 0;
+    touch(q, v);
+    mark_dirty(q, g.V, v, i, 0, 0);
+  }
+  (void)L;
+}
+
+// Base states: cost 0 for every S inside groupset(v) (CPUNONHOP.h:594-624).
+__global__ void k_init_base(Slot* slots, int t, Graph g) {
+  Slot& q = slots[t];
+  const int k = q.k, W = q.W, L = q.L, rowlen = W * L;
+  const int n = q.ntouched;
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
+    uint32_t v = q.touched[x];
+    int32_t* row = q.table + (long long)v * rowlen;
+    int gs = 0;
+    for (int i = 0; i < k; ++i)
+      if (row[(1 + i) * L] == 0) gs |= 1 << i;
+    for (int S = gs; S > 0; S = (S - 1) & gs)
+      if (__popc(S) >= 2) row[c_sub.sidx[k][S] * L] = 0;
+    if (gs == W - 1) atomicMin(&q.best, 0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Control: advance every slot's state machine and lay out this round's work.
+// One block of MAXSLOTS threads.
+// ---------------------------------------------------------------------------
+__global__ void k_ctl_a(Slot* slots, int nslots, Plan* plan, SlotStatus* status) {
+  __shared__ long long s_scan[2][MAXSLOTS];
+  __shared__ int s_cnt[3][MAXSLOTS];
+  const int t = threadIdx.x;
+  int act = A_NONE;
+  long long n_merge = 0, n_prep = 0;
+  if (t < nslots) {
+    Slot& q = slots[t];
+    if (q.phase == PH_ACTIVE) {
+      const bool hop = q.D >= 0;
+      const int pa = q.action;
+      q.rounds++;
+      if (q.err != ERR_NONE || (q.max_rounds > 0 && q.rounds > q.max_rounds)) {
+        if (q.err == ERR_NONE) q.err = ERR_ROUNDS;
+        q.phase = PH_ERROR;
+      } else {
+        bool done = false;
+        switch (pa) {
+          case A_INIT: if (!hop) q.cur ^= 1; else q.d = 0; break;
+          case A_GROW:
+            if (!hop) { q.qcount[q.cur] = 0; q.cur ^= 1; }
+            else { q.qcount[q.d] = 0; q.d += 1; }
+            break;
+          case A_MERGE: if (!hop) q.cur ^= 1; else q.d = 0; break;
+          case A_MERGEFULL: q.phase = PH_DONE; done = true; break;
+          default: break;
+        }
+        q.nchunks = 0;
+        if (!done) {
+          if (pa == A_LBPREP) {
+            q.s = 2;
+            act = (q.k == 2) ? A_MERGEFULL : A_MERGE;
+          } else {
+            bool more;
+            if (!hop) {
+              more = q.qcount[q.cur] > 0;
+            } else {
+              while (q.d < q.D && q.qcount[q.d] == 0) q.d++;
+              more = q.d < q.D;
+            }
+            if (more) {
+              act = A_GROW;
+            } else if (q.s == 1) {
+              act = A_LBPREP;
+            } else {
+              q.s += 1;
+              act = (q.s == q.k) ? A_MERGEFULL : A_MERGE;
+            }
+          }
+          if (act == A_MERGE || act == A_MERGEFULL) n_merge = q.ntouched;
+          if (act == A_GROW) n_prep = hop ? q.qcount[q.d] : q.qcount[q.cur];
+        }
+      }
+      q.action = act;
+    }
+    status[t].phase = q.phase;
+    status[t].err = q.err;
+    status[t].answer = q.answer;
+  }
+  // compact the slot list of each action with block-wide inclusive scans
+  const int f0 = (act == A_LBPREP), f1 = (act == A_MERGE || act == A_MERGEFULL), f2 = (act == A_GROW);
+  s_cnt[0][t] = f0;
+  s_cnt[1][t] = f1;
+  s_cnt[2][t] = f2;
+  s_scan[0][t] = f1 ? n_merge : 0;
+  s_scan[1][t] = f2 ? n_prep : 0;
+  __syncthreads();
+  for (int off = 1; off < MAXSLOTS; off <<= 1) {
+    long long a0 = 0, a1 = 0;
+    int c0 = 0, c1 = 0, c2 = 0;
+    if (t >= off) {
+      a0 = s_scan[0][t - off]; a1 = s_scan[1][t - off];
+      c0 = s_cnt[0][t - off]; c1 = s_cnt[1][t - off]; c2 = s_cnt[2][t - off];
+    }
+    __syncthreads();
+    s_scan[0][t] += a0; s_scan[1][t] += a1;
+    s_cnt[0][t] += c0; s_cnt[1][t] += c1; s_cnt[2][t] += c2;
+    __syncthreads();
+  }
+  if (f0) plan->lb_slots[s_cnt[0][t] - 1] = t;
+  if (f1) {
+    const int p = s_cnt[1][t] - 1;
+    plan->merge_slots[p] = t;
+    plan->merge_off[p] = s_scan[0][t] - n_merge;
+  }
+  if (f2) {
+    const int p = s_cnt[2][t] - 1;
+    plan->grow_slots[p] = t;
+    plan->prep_off[p] = s_scan[1][t] - n_prep;
+  }
+  if (t == MAXSLOTS - 1) {
+    plan->n_lb = s_cnt[0][t];
+    plan->n_merge = s_cnt[1][t];
+    plan->n_grow = s_cnt[2][t];
+    plan->merge_off[s_cnt[1][t]] = s_scan[0][t];
+    plan->prep_off[s_cnt[2][t]] = s_scan[1][t];
+  }
+}
+
+// Chunk offsets of the grow slots, after the prep pass.
+__global__ void k_ctl_b(Slot* slots, Plan* plan) {
+  __shared__ long long s_scan[MAXSLOTS];
+  const int t = threadIdx.x;
+  const int n = plan->n_grow;
+  long long c = 0;
+  if (t < n) {
+    Slot& q = slots[plan->grow_slots[t]];
+    c = q.nchunks;
+    if (c > q.chunk_cap) { q.err = ERR_CHUNK_CAP; c = 0; }
+  }
+  s_scan[t] = c;
+  __syncthreads();
+  for (int off = 1; off < MAXSLOTS; off <<= 1) {
+    long long a = t >= off ? s_scan[t - off] : 0;
+    __syncthreads();
+    s_scan[t] += a;
+    __syncthreads();
+  }
+  if (t < n) plan->chunk_off[t] = s_scan[t] - c;
+  if (t == MAXSLOTS - 1) plan->chunk_off[n] = s_scan[t];
+}
+
+// ---------------------------------------------------------------------------
+// Lower-bound tables after the singleton layer (one block per slot).
+// vv[i][j]  lower bound of dist(g_i, g_j) from the clipped singleton distances
+//           of the members of g_i (virtual_node_distances, CPUNONHOP.h:175-210);
+// P[i][j][X] cheapest visiting order of the groups of X from i to j (Held-Karp
+//           over vv, the W table of CPUNONHOP.h:269-386 / DPQ.cu:445-472);
+// W2[i][X]  min over j of P[i][j][X] (CPUNONHOP.h:568-587).
+// ---------------------------------------------------------------------------
+__global__ void k_lbprep(Slot* slots, const Plan* plan, Graph g) {
+  __shared__ int s_vv[MAXK * MAXK];
+  __shared__ int s_P[MAXK * MAXK * MAXW];
+  for (int j = blockIdx.x; j < plan->n_lb; j += gridDim.x) {
+    Slot& q = slots[plan->lb_slots[j]];
+    const int k = q.k, W = q.W, L = q.L, rowlen = W * L;
+    const int R1 = q.best >= INF ? INF / 2 : q.best / 2;
+    __syncthreads();
+    for (int x = threadIdx.x; x < k * k; x += blockDim.x) s_vv[x] = INF;
+    for (int x = threadIdx.x; x < k * k * W; x += blockDim.x) s_P[x] = INF;
+    __syncthreads();
+    for (int i = 0; i < k; ++i) {
+      const long long b = g.gptr[q.groups[i]], e = g.gptr[q.groups[i] + 1];
+      for (long long m = b + threadIdx.x; m < e; m += blockDim.x) {
+        const int32_t* row = q.table + (long long)g.gmem[m] * rowlen;
+        for (int jj = 0; jj < k; ++jj) {
+          int dmin = INF;
+          for (int l = 0; l < L; ++l) dmin = imin(dmin, row[(1 + jj) * L + l]);
+          atomicMin(&s_vv[i * k + jj], clip_dist(dmin, R1));
+        }
+      }
+    }
+    __syncthreads();
+    {  // both directions bound the same distance
+      int a = 0, b = 0;
+      if (threadIdx.x < k * k) {
+        a = s_vv[threadIdx.x];
+        b = s_vv[(threadIdx.x % k) * k + threadIdx.x / k];
+      }
+      __syncthreads();
+      if (threadIdx.x < k * k) s_vv[threadIdx.x] = imax(a, b);
+    }
+    if (threadIdx.x < k) s_P[(threadIdx.x * k + threadIdx.x) * W + (1 << threadIdx.x)] = 0;
+    __syncthreads();
+    for (int X = 1; X < W; ++X) {
+      for (int x = threadIdx.x; x < k * k; x += blockDim.x) {
+        int i = x / k, jj = x % k;
+        if (!((X >> i) & 1) || !((X >> jj) & 1)) continue;
+        int cur = s_P[(i * k + jj) * W + X];
+        if (cur >= INF) continue;
+        for (int l = 0; l < k; ++l) {
+          if ((X >> l) & 1) continue;
+          int cand = cur + s_vv[jj * k + l];
+          if (cand < INF) atomicMin(&s_P[(i * k + l) * W + (X | (1 << l))], cand);
+        }
+      }
+      __syncthreads();
+    }
+    for (int x = threadIdx.x; x < k * k * W; x += blockDim.x) q.lbtab[x] = s_P[x];
+    for (int x = threadIdx.x; x < k * W; x += blockDim.x) {
+      int i = x / W, X = x % W;
+      int m = INF;
+      for (int jj = 0; jj < k; ++jj) m = imin(m, s_P[(i * k + jj) * W + X]);
+      q.lbtab[k * k * W + x] = m;
+    }
+    if (threadIdx.x == 0) q.R1 = R1;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Merge: subset join of layer s at every touched vertex (one warp per vertex,
+// the vertex's row staged in shared memory).
+// ---------------------------------------------------------------------------
+constexpr int MERGE_WARPS = 8;
+
+__global__ void __launch_bounds__(MERGE_WARPS * 32)
+k_merge(Slot* slots, const Plan* plan, Graph g) {
+  extern __shared__ int s_rows[];  // MERGE_WARPS x (MAXW * MAXL)
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  int* srow = s_rows + wib * (MAXW * MAXL);
+  const int nm = plan->n_merge;
+  if (nm == 0) return;
+  const long long total = plan->merge_off[nm];
+  const long long nwarps = (long long)gridDim.x * MERGE_WARPS;
+  for (long long gi = blockIdx.x * (long long)MERGE_WARPS + wib; gi < total; gi += nwarps) {
+    const int j = seg_search(plan->merge_off, nm, gi);
+    Slot& q = slots[plan->merge_slots[j]];
+    const uint32_t v = q.touched[gi - plan->merge_off[j]];
+    const int k = q.k, W = q.W, L = q.L, rowlen = W * L, D = q.D, s = q.s;
+    const bool hop = D >= 0;
+    const int best = *(volatile int*)&q.best;
+    const int R1 = q.R1;
+    int32_t* vrow = q.table + (long long)v * rowlen;
+    // stage the row; raw values kept in registers for the layer's own sets
+    for (int x = lane; x < rowlen; x += 32) srow[x] = vrow[x];
+    __syncwarp();
+    if (hop) {  // prefix minima over labels
+      for (int x = lane; x < W; x += 32) {
+        int m = INF;
+        for (int l = 0; l < L; ++l) {
+          m = imin(m, srow[x * L + l]);
+          srow[x * L + l] = m;
+        }
+      }
+      __syncwarp();
+    }
+    int dist[MAXK];
+    for (int i = 0; i < k; ++i) dist[i] = clip_dist(srow[(1 + i) * L + (L - 1)], R1);
+    const int lo = c_sub.loff[k][s], nS = c_sub.loff[k][s + 1] - lo;
+    unsigned long long nmerge = 0;
+    for (int r = lane; r < nS; r += 32) {
+      const int S = c_sub.sof[k][lo + r];
+      int M[MAXL];
+      for (int l = 0; l < L; ++l) M[l] = srow[(lo + r) * L + l];
+      for (int S1 = (S - 1) & S; S1 > 0; S1 = (S1 - 1) & S) {
+        const int S2 = S ^ S1;
+        if (S1 < S2) continue;
+        const int i1 = c_sub.sidx[k][S1] * L, i2 = c_sub.sidx[k][S2] * L;
+        ++nmerge;
+        if (!hop) {
+          M[0] = imin(M[0], srow[i1] + srow[i2]);
+        } else {
+          for (int l = 0; l < L; ++l) {
+            const int m2 = imin(l, D - l);
+            const int c = imin(srow[i1 + l] + srow[i2 + m2], srow[i1 + m2] + srow[i2 + l]);
+            M[l] = imin(M[l], c);
+          }
+        }
+      }
+      for (int l = 1; l < L; ++l) M[l] = imin(M[l], M[l - 1]);
+      if (s == k) {
+        const int ans = M[L - 1];
+        if (ans < INF)
+          atomicMin(&q.answer, ((unsigned long long)(unsigned)ans << 32) | (unsigned long long)v);
+        continue;
+      }
+      const int lbv = lower_bound(dist, k, W, S, q.lbtab);
+      for (int l = 0; l < L; ++l) {
+        const int val = M[l];
+        if (val >= INF) continue;
+        if (l > 0 && val >= M[l - 1]) continue;      // no better than a smaller label
+        if ((long long)val + lbv > best) continue;   // cannot be part of an optimum
+        const long long idx = (long long)(lo + r) * L + l;
+        if (val < vrow[idx]) vrow[idx] = val;
+        // star upper bound: join the cheapest path to every missing group
+        long long ub = val;
+        const int hl = hop ? imin(l, D - l) : 0;
+        for (int i = 0; i < k && ub < INF; ++i)
+          if (!((S >> i) & 1)) ub += srow[(1 + i) * L + hl];
+        if (ub < best) atomicMin(&q.best, (int)ub);
+        if (2LL * val <= best && (!hop || l < D)) mark_dirty(q, g.V, v, r, hop ? l : 0, hop ? l : (q.cur ^ 1));
+      }
+    }
+    for (int o = 16; o; o >>= 1) nmerge += __shfl_down_sync(0xffffffffu, nmerge, o);
+    if (lane == 0 && nmerge) atomicAdd(&q.st_merges, nmerge);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Prep: snapshot the dirty masks of this round's frontier and cut each
+// vertex's adjacency into chunks of bounded work.
+// ---------------------------------------------------------------------------
+__global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
+  const int ng = plan->n_grow;
+  if (ng == 0) return;
+  const long long total = plan->prep_off[ng];
+  for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < total;
+       gi += (long long)gridDim.x * blockDim.x) {
+    const int j = seg_search(plan->prep_off, ng, gi);
+    Slot& q = slots[plan->grow_slots[j]];
+    const bool hop = q.D >= 0;
+    const int lvl = hop ? q.d : 0;
+    const int qi = hop ? q.d : q.cur;
+    const uint32_t v = q.queue[(long long)qi * g.V + (gi - plan->prep_off[j])];
+    const unsigned long long m = atomicExch(&q.mask[(long long)lvl * g.V + v], 0ull);
+    if (m == 0ull) continue;
+    const long long eb = g.rowptr[v], ee = g.rowptr[v + 1];
+    const int nb = __popcll(m);
+    atomicAdd(&q.st_frontier, (unsigned long long)nb);
+    if (ee == eb) continue;
+    const long long ch = imax(32, 1024 / nb);
+    const int nch = (int)((ee - eb + ch - 1) / ch);
+    const int pos = atomicAdd(&q.nchunks, nch);
+    if (pos + nch > q.chunk_cap) { q.err = ERR_CHUNK_CAP; continue; }
+    for (int c = 0; c < nch; ++c) {
+      Chunk x;
+      x.v = v;
+      x.eb = (uint32_t)(eb + c * ch);
+      x.ee = (uint32_t)(eb + (c + 1) * ch < ee ? eb + (c + 1) * ch : ee);
+      x.pad = 0;
+      x.mask = m;
+      q.chunks[pos + c] = x;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Grow: one warp per chunk.  Lanes walk (edge, dirty set) pairs with the set
+// index fastest, so the lanes relaxing one neighbour touch adjacent words of
+// its row.  A target is read before the atomicMin and the lower bound is only
+// evaluated for candidates that improve it.
+// ---------------------------------------------------------------------------
+constexpr int GROW_WARPS = 8;
+
+__global__ void __launch_bounds__(GROW_WARPS * 32)
+k_grow(Slot* slots, const Plan* plan, Graph g) {
+  __shared__ int s_r[GROW_WARPS][64];
+  __shared__ int s_sv[GROW_WARPS][64];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int ng = plan->n_grow;
+  if (ng == 0) return;
+  const long long total = plan->chunk_off[ng];
+  const long long nwarps = (long long)gridDim.x * GROW_WARPS;
+  for (long long gi = blockIdx.x * (long long)GROW_WARPS + wib; gi < total; gi += nwarps) {
+    const int j = seg_search(plan->chunk_off, ng, gi);
+    Slot& q = slots[plan->grow_slots[j]];
+    const Chunk c = q.chunks[gi - plan->chunk_off[j]];
+    const int k = q.k, W = q.W, L = q.L, rowlen = W * L, D = q.D, s = q.s;
+    const bool hop = D >= 0;
+    const int d = hop ? q.d : 0;
+    const int td = hop ? d + 1 : 0;
+    const int best = *(volatile int*)&q.best;
+    const int R1 = q.R1;
+    const int lo = c_sub.loff[k][s];
+    const int32_t* src = q.table + (long long)c.v * rowlen;
+    // dirty sets whose source cost is still a valid grow source
+    int nact = 0;
+    for (int base = 0; base < 64; base += 32) {
+      const int b = base + lane;
+      int r = -1, sv = INF;
+      if ((c.mask >> b) & 1ull) {
+        r = b;
+        sv = src[(lo + r) * L + d];
+        if (sv >= INF || 2LL * sv > best) r = -1;
+      }
+      const unsigned ok = __ballot_sync(0xffffffffu, r >= 0);
+      if (r >= 0) {
+        const int p = nact + __popc(ok & ((1u << lane) - 1));
+        s_r[wib][p] = r;
+        s_sv[wib][p] = sv;
+      }
+      nact += __popc(ok);
+    }
+    __syncwarp();
+    unsigned long long nrel = 0, nimp = 0;
+    if (nact > 0) {
+      const long long npairs = (long long)(c.ee - c.eb) * nact;
+      for (long long p = lane; p < npairs; p += 32) {
+        const long long e = c.eb + p / nact;
+        const int bi = (int)(p % nact);
+        const int2 a = __ldg(&g.adj[e]);
+        const uint32_t u = (uint32_t)a.x;
+        const int nc = s_sv[wib][bi] + a.y;
+        ++nrel;
+        if (nc >= INF) continue;
+        const int r = s_r[wib][bi];
+        int32_t* trow = q.table + (long long)u * rowlen;
+        const long long tidx = (long long)(lo + r) * L;
+        int cur = trow[tidx + td];
+        for (int l = 0; l < td; ++l) cur = imin(cur, trow[tidx + l]);
+        if (nc >= cur) continue;
+        if (s >= 2) {
+          int dist[MAXK];
+          for (int i = 0; i < k; ++i) {
+            int dm = INF;
+            for (int l = 0; l < L; ++l) dm = imin(dm, trow[(1 + i) * L + l]);
+            dist[i] = clip_dist(dm, R1);
+          }
+          const int S = c_sub.sof[k][lo + r];
+          if ((long long)nc + lower_bound(dist, k, W, S, q.lbtab) > best) continue;
+        }
+        const int old = atomicMin(&trow[tidx + td], nc);
+        if (old <= nc) continue;
+        ++nimp;
+        touch(q, u);
+        if (s == 1) {  // star upper bound from a vertex that reaches every group
+          long long ub = 0;
+          const int hl = hop ? D / 2 : 0;
+          if (!hop || td <= hl) {
+            for (int i = 0; i < k && ub < INF; ++i) {
+              int dm = INF;
+              for (int l = 0; l <= hl; ++l) dm = imin(dm, trow[(1 + i) * L + l]);
+              ub += dm;
+            }
+            if (ub < best) atomicMin(&q.best, (int)ub);
+          }
+        }
+        if (2LL * nc <= best && (!hop || td < D))
+          mark_dirty(q, g.V, u, r, hop ? td : 0, hop ? td : (q.cur ^ 1));
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      nrel += __shfl_down_sync(0xffffffffu, nrel, o);
+      nimp += __shfl_down_sync(0xffffffffu, nimp, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&q.st_relax, nrel);
+      if (nimp) atomicAdd(&q.st_improve, nimp);
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Witness search: rebuild the tree of a finished slot from its table (one
+// block per slot).  Every step follows an exact equality (base, smaller label,
+// merge split or grow edge), so the walk ends at base states; a bounded stack
+// turns any inconsistency into ERR_WITNESS instead of a hang.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int cum_at(const int32_t* row, int idx, int L, int l) {
+  int m = INF;
+  for (int x = 0; x <= l; ++x) m = imin(m, row[idx * L + x]);
+  return m;
+}
+
+__global__ void k_witness(Slot* slots, const int* list, int n, Graph g) {
+  __shared__ int s_top, s_found, s_fu, s_stop;
+  __shared__ int s_x, s_S, s_l, s_C;
+  for (int j = blockIdx.x; j < n; j += gridDim.x) {
+    Slot& q = slots[list[j]];
+    const int k = q.k, W = q.W, L = q.L, rowlen = W * L, D = q.D;
+    const bool hop = D >= 0;
+    const int full = W - 1;
+    if (threadIdx.x == 0) {
+      s_top = 0;
+      s_stop = 0;
+      q.nwedges = 0;
+      const unsigned long long a = q.answer;
+      q.wstack[0] = (int)(a & 0xffffffffu);
+      q.wstack[1] = full;
+      q.wstack[2] = L - 1;
+      q.wstack[3] = (int)(a >> 32);
+      s_top = 1;
+    }
+    __syncthreads();
+    long long steps = 0;
+    while (true) {
+      if (threadIdx.x == 0) {
+        if (s_top == 0 || s_stop) {
+          s_x = -1;
+        } else {
+          --s_top;
+          s_x = q.wstack[s_top * 4 + 0];
+          s_S = q.wstack[s_top * 4 + 1];
+          s_l = q.wstack[s_top * 4 + 2];
+          s_C = q.wstack[s_top * 4 + 3];
+        }
+        s_found = 0;
+      }
+      __syncthreads();
+      if (s_x < 0) break;
+      if (++steps > 8 * q.wcap) {
+        if (threadIdx.x == 0) { q.err = ERR_WITNESS_CAP; s_stop = 1; }
+        __syncthreads();
+        continue;
+      }
+      const int x = s_x, S = s_S, l = s_l, C = s_C;
+      const int32_t* row = q.table + (long long)x * rowlen;
+      if (threadIdx.x == 0) {
+        int gs = 0;
+        for (int i = 0; i < k; ++i)
+          if (row[(1 + i) * L] == 0) gs |= 1 << i;
+        int found = 0;
+        if (C == 0 && (S & gs) == S) {
+          found = 1;  // base state
+        } else if (hop && l > 0 && S != full && cum_at(row, c_sub.sidx[k][S], L, l - 1) == C) {
+          found = 2;
+          if (s_top + 1 > q.wcap) { q.err = ERR_WITNESS_CAP; s_stop = 1; }
+          else {
+            int* st = q.wstack + s_top * 4;
+            st[0] = x; st[1] = S; st[2] = l - 1; st[3] = C;
+            ++s_top;
+          }
+        } else {
+          // merge witness at label l; the full set is not stored, so its root
+          // may have been joined at any label up to l
+          const int lmin = (hop && S == full) ? 0 : l;
+          for (int S1 = (S - 1) & S; S1 > 0 && !found; S1 = (S1 - 1) & S) {
+            const int S2 = S ^ S1;
+            if (S1 < S2) continue;
+            const int i1 = c_sub.sidx[k][S1], i2 = c_sub.sidx[k][S2];
+            int l1 = 0, l2 = 0, c1 = INF, c2 = INF;
+            if (!hop) {
+              c1 = row[i1]; c2 = row[i2];
+            } else {
+              for (int lj = lmin; lj <= l && c1 >= INF; ++lj) {
+                const int m2 = imin(lj, D - lj);
+                const int a1 = cum_at(row, i1, L, lj), a2 = cum_at(row, i2, L, m2);
+                const int b1 = cum_at(row, i1, L, m2), b2 = cum_at(row, i2, L, lj);
+                if (a1 < INF && a2 < INF && a1 + a2 == C) { c1 = a1; c2 = a2; l1 = lj; l2 = m2; }
+                else if (b1 < INF && b2 < INF && b1 + b2 == C) { c1 = b1; c2 = b2; l1 = m2; l2 = lj; }
+              }
+            }
+            if (c1 < INF && c2 < INF && c1 + c2 == C) {
+              found = 3;
+              if (s_top + 2 > q.wcap) { q.err = ERR_WITNESS_CAP; s_stop = 1; }
+              else {
+                int* st = q.wstack + s_top * 4;
+                st[0] = x; st[1] = S1; st[2] = l1; st[3] = c1;
+                st[4] = x; st[5] = S2; st[6] = l2; st[7] = c2;
+                s_top += 2;
+              }
+            }
+          }
+        }
+        s_found = found;
+        s_fu = INT32_MAX;
+      }
+      __syncthreads();
+      if (s_found == 0 && S != full && (!hop || l > 0)) {
+        // grow witness: a neighbour u with cost(u, S, l-1) + w == C
+        const int idx = c_sub.sidx[k][S];
+        const long long eb = g.rowptr[x], ee = g.rowptr[x + 1];
+        for (long long e = eb + threadIdx.x; e < ee; e += blockDim.x) {
+          const int2 a = g.adj[e];
+          if (a.y > C) continue;
+          const int32_t* urow = q.table + (long long)a.x * rowlen;
+          const int cu = hop ? cum_at(urow, idx, L, l - 1) : urow[idx];
+          if (cu < INF && cu + a.y == C) atomicMin(&s_fu, (int)(e - eb));
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          if (s_fu != INT32_MAX) {
+            const int2 a = g.adj[eb + s_fu];
+            if (s_top + 1 > q.wcap || q.nwedges + 1 > q.wcap) { q.err = ERR_WITNESS_CAP; s_stop = 1; }
+            else {
+              int* st = q.wstack + s_top * 4;
+              st[0] = a.x; st[1] = S; st[2] = hop ? l - 1 : 0; st[3] = C - a.y;
+              ++s_top;
+              int* oe = q.wedges + q.nwedges * 3;
+              oe[0] = x; oe[1] = a.x; oe[2] = a.y;
+              q.nwedges++;
+            }
+          } else {
+            q.err = ERR_WITNESS;
+            s_stop = 1;
+          }
+        }
+      } else if (s_found == 0 && threadIdx.x == 0) {
+        q.err = ERR_WITNESS;
+        s_stop = 1;
+      }
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+}
+
+// Publishes every slot's status after a batch of rounds.  A slot whose full
+// merge ran in the last round is finished here (the transition the next
+// control pass would make).
+__global__ void k_publish(Slot* slots, int nslots, SlotStatus* status) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nslots) return;
+  Slot& q = slots[t];
+  if (q.phase == PH_ACTIVE && q.action == A_MERGEFULL && q.err == ERR_NONE) {
+    q.phase = PH_DONE;
+    q.action = A_NONE;
+  }
+  status[t].phase = q.phase;
+  status[t].err = q.err;
+  status[t].answer = q.answer;
+}
+
+__global__ void k_free_slot(Slot* slots, int t) {
+  slots[t].phase = PH_FREE;
+  slots[t].action = A_NONE;
+}
+
+// Resets the rows and flags of a finished slot so its slab can be reused.
+__global__ void k_reset(Slot* slots, int t, Graph g) {
+  Slot& q = slots[t];
+  const int rowlen = q.W * q.L, L = q.L;
+  const int n = q.ntouched;
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < (long long)n * rowlen;
+       x += (long long)gridDim.x * blockDim.x) {
+    const uint32_t v = q.touched[x / rowlen];
+    q.table[(long long)v * rowlen + (x % rowlen)] = INF;
+  }
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < (long long)n * L;
+       x += (long long)gridDim.x * blockDim.x) {
+    const uint32_t v = q.touched[x / L];
+    q.mask[(x % L) * g.V + v] = 0ull;
+    if (x % L == 0) q.tflag[v] = 0u;
+  }
+}
+
+}  // namespace gst

@@ -1,0 +1,71 @@
+"""The oracle restatement against the reference's own outputs (CPU only).
+
+The fixtures hold what the reference PrunedDP++ / D-PrunedDP++ binaries
+printed on seeded inputs (tests/golden/make_golden.py); the oracle must
+reproduce every cost, and its trees must validate.  The unpruned exact DPBF
+must agree too, which shows the reference's pruning kept the optimum."""
+import numpy as np
+import pytest
+
+import oracle
+
+
+@pytest.mark.parametrize("name", ["toy60", "s3000", "c1", "edge"])
+def test_prunedpp_restatement_matches_reference(golden, name):
+    fx, g, gr = golden(name)
+    for k, qs in fx["queries"].items():
+        want = fx["reference"]["prunedpp"][k]
+        assert len(want) == len(qs)
+        for ids, w in zip(qs, want):
+            cost, edges, root, _ = oracle.prunedpp(g, gr, ids)
+            assert cost == w, (name, ids, cost, w)
+            if cost < oracle.INF:
+                assert oracle.validate(g, gr, ids, edges, root, cost) == 0
+
+
+@pytest.mark.parametrize("name", ["toy60", "s3000", "edge"])
+def test_unpruned_dpbf_matches_reference(golden, name):
+    fx, g, gr = golden(name)
+    for k, qs in fx["queries"].items():
+        for ids, w in zip(qs, fx["reference"]["prunedpp"][k]):
+            cost, edges, root, _ = oracle.dpbf(g, gr, ids)
+            assert cost == w, (name, ids, cost, w)
+            if cost < oracle.INF:
+                assert oracle.validate(g, gr, ids, edges, root, cost) == 0
+
+
+@pytest.mark.parametrize("name", ["toy60", "s3000", "c1", "edge"])
+def test_hop_restatement_matches_reference(golden, name):
+    fx, g, gr = golden(name)
+    for h in fx["reference"]["hop"]:
+        qs = fx["queries"][str(h["k"])][: h["n"]]
+        for ids, w in zip(qs, h["costs"]):
+            cost, edges, root, _ = oracle.hop(g, gr, ids, h["D"])
+            assert cost == w, (name, ids, h["D"], cost, w)
+
+
+def test_hop_properties_on_oracle(golden):
+    """Cost is non-increasing in D and reaches the plain optimum for large D."""
+    fx, g, gr = golden("toy60")
+    for ids in fx["queries"]["3"][:8]:
+        plain = oracle.dpbf(g, gr, ids)[0]
+        prev = None
+        for D in range(0, 8):
+            c = oracle.hop(g, gr, ids, D)[0]
+            if prev is not None:
+                assert c <= prev
+            prev = c
+        assert oracle.hop(g, gr, ids, 59)[0] == plain
+
+
+def test_validator_rejects_bad_trees(golden):
+    fx, g, gr = golden("toy60")
+    ids = fx["queries"]["3"][0]
+    cost, edges, root, _ = oracle.prunedpp(g, gr, ids)
+    assert oracle.validate(g, gr, ids, edges, root, cost) == 0
+    assert oracle.validate(g, gr, ids, edges, root, cost + 1) == 4       # wrong weight
+    if len(edges) > 1:
+        assert oracle.validate(g, gr, ids, edges[1:], root, cost) != 0   # cover/connectivity
+    bad = edges.copy()
+    bad[0, 2] += 1
+    assert oracle.validate(g, gr, ids, bad, root, cost) == 1              # weight mismatch
