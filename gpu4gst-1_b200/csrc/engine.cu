@@ -149,6 +149,7 @@ class Engine {
     device_ = c.device;
     max_slots_ = c.max_slots > 0 ? std::min(c.max_slots, MAXSLOTS) : 256;
     max_rounds_override_ = c.max_rounds > 0 ? c.max_rounds : 0;
+    profile_ = c.profile != 0;
     rounds_per_poll_ = c.rounds_per_poll > 0 ? c.rounds_per_poll : 8;
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
@@ -309,6 +310,12 @@ class Engine {
     std::lock_guard<std::mutex> lk(mu_);
     if (busy_) return fail(GST_E_STATE, "engine is serving; use the server API");
     GST_CUDA(cudaSetDevice(device_));
+    if (!ev_run0_) {
+      GST_CUDA(cudaEventCreate(&ev_run0_));
+      GST_CUDA(cudaEventCreate(&ev_run1_));
+    }
+    std::memset(&prof_, 0, sizeof prof_);
+    GST_CUDA(cudaEventRecord(ev_run0_, stream_));
     for (auto& r : reqs)
       if (r && !r->done) pending_.push_back(r);
     while (true) {
@@ -316,8 +323,15 @@ class Engine {
       if (s != GST_OK) return s;
       if (pending_.empty() && active_ == 0) break;
     }
+    GST_CUDA(cudaEventRecord(ev_run1_, stream_));
+    GST_CUDA(cudaEventSynchronize(ev_run1_));
+    float ms = 0;
+    GST_CUDA(cudaEventElapsedTime(&ms, ev_run0_, ev_run1_));
+    prof_.run_ms = ms;
     return GST_OK;
   }
+
+  gst_profile profile() const { return prof_; }
 
   // One scheduling step: admit, run rounds_per_poll rounds, harvest.
   gst_status step() {
@@ -464,9 +478,12 @@ class Engine {
     s.off = off;
     s.bytes = bytes;
     const size_t V = (size_t)V_, W = (size_t)1 << sh.k, L = (size_t)sh.L;
-    cudaMemsetAsync(s.table, 0x3f, V * W * L * 4, stream_);
-    cudaMemsetAsync(s.mask, 0, L * V * 8, stream_);
-    cudaMemsetAsync(s.tflag, 0, V * 4, stream_);
+    if (cudaMemsetAsync(s.table, 0x3f, V * W * L * 4, stream_) != cudaSuccess ||
+        cudaMemsetAsync(s.mask, 0, L * V * 8, stream_) != cudaSuccess ||
+        cudaMemsetAsync(s.tflag, 0, V * 4, stream_) != cudaSuccess) {
+      arena_alloc_.release(off, bytes);
+      return false;
+    }
     *out = s;
     return true;
   }
@@ -519,13 +536,15 @@ class Engine {
       q.R1 = INF / 2;
       q.answer = ~0ull;
       GST_CUDA(cudaMemcpyAsync(d_slots_ + t, &q, sizeof(Slot), cudaMemcpyHostToDevice, stream_));
+      prof_.h2d_bytes += sizeof(Slot);
       GST_CUDA(cudaStreamSynchronize(stream_));  // h_slot_ is reused
-      if (!r->t0) cudaEventCreate(&r->t0);
-      cudaEventRecord(r->t0, stream_);
+      if (!r->t0) GST_CUDA(cudaEventCreate(&r->t0));
+      GST_CUDA(cudaEventRecord(r->t0, stream_));
       Graph g = graph();
       k_init_seeds<<<64, 256, 0, stream_>>>(d_slots_, t, g);
       k_init_base<<<64, 256, 0, stream_>>>(d_slots_, t, g);
       GST_CUDA(cudaGetLastError());
+      prof_.kernel_launches += 2;
       slot_busy_[t] = 1;
       slot_req_[t] = r;
       slot_slab_[t] = sb;
@@ -547,15 +566,19 @@ class Engine {
     return g;
   }
 
-  void enqueue_round(cudaStream_t st) {
+  void enqueue_round(cudaStream_t st, int i) {
     Graph g = graph();
     const int grid = num_sms_ * 4;
     k_ctl_a<<<1, MAXSLOTS, 0, st>>>(d_slots_, max_slots_, d_plan_, d_status_);
     k_lbprep<<<std::min(max_slots_, 256), 256, 0, st>>>(d_slots_, d_plan_, g);
+    if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 0], st, cudaEventRecordExternal);
     k_merge<<<grid, MERGE_WARPS * 32, MERGE_WARPS * MAXW * MAXL * sizeof(int), st>>>(d_slots_, d_plan_, g);
+    if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 1], st, cudaEventRecordExternal);
     k_prep<<<grid, 256, 0, st>>>(d_slots_, d_plan_, g);
     k_ctl_b<<<1, MAXSLOTS, 0, st>>>(d_slots_, d_plan_);
+    if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 2], st, cudaEventRecordExternal);
     k_grow<<<grid, GROW_WARPS * 32, 0, st>>>(d_slots_, d_plan_, g);
+    if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 3], st, cudaEventRecordExternal);
   }
 
   gst_status launch_rounds() {
@@ -563,8 +586,13 @@ class Engine {
       if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
       graph_exec_ = nullptr;
       cudaGraph_t gr;
+      if (profile_) {
+        for (auto ev : ev_prof_) if (ev) cudaEventDestroy(ev);
+        ev_prof_.assign(4 * rounds_per_poll_, nullptr);
+        for (auto& ev : ev_prof_) GST_CUDA(cudaEventCreate(&ev));
+      }
       GST_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-      for (int i = 0; i < rounds_per_poll_; ++i) enqueue_round(stream_);
+      for (int i = 0; i < rounds_per_poll_; ++i) enqueue_round(stream_, i);
       GST_CUDA(cudaStreamEndCapture(stream_, &gr));
       GST_CUDA(cudaGraphInstantiate(&graph_exec_, gr, 0));
       cudaGraphDestroy(gr);
@@ -576,6 +604,20 @@ class Engine {
     GST_CUDA(cudaMemcpyAsync(h_status_, d_status_, sizeof(SlotStatus) * max_slots_,
                              cudaMemcpyDeviceToHost, stream_));
     GST_CUDA(cudaStreamSynchronize(stream_));
+    prof_.rounds += rounds_per_poll_;
+    prof_.kernel_launches += 6 * rounds_per_poll_ + 1;
+    prof_.d2h_bytes += sizeof(SlotStatus) * max_slots_;
+    if (profile_) {
+      for (int i = 0; i < rounds_per_poll_; ++i) {
+        float a = 0, b = 0;
+        GST_CUDA(cudaEventElapsedTime(&a, ev_prof_[4 * i + 0], ev_prof_[4 * i + 1]));
+        GST_CUDA(cudaEventElapsedTime(&b, ev_prof_[4 * i + 2], ev_prof_[4 * i + 3]));
+        prof_.merge_ms += a;
+        prof_.grow_ms += b;
+      }
+      prof_.merge_launches += rounds_per_poll_;
+      prof_.grow_launches += rounds_per_poll_;
+    }
     return GST_OK;
   }
 
@@ -586,8 +628,9 @@ class Engine {
         fin.push_back(t);
     if (fin.empty()) return GST_OK;
     cudaEvent_t t1;
-    cudaEventCreate(&t1);
-    cudaEventRecord(t1, stream_);
+    GST_CUDA(cudaEventCreate(&t1));
+    GST_CUDA(cudaEventRecord(t1, stream_));
+    GST_CUDA(cudaEventSynchronize(t1));
     std::vector<int> wit;
     for (int t : fin)
       if (h_status_[t].phase == PH_DONE && (h_status_[t].answer >> 32) < (unsigned long long)INF)
@@ -598,17 +641,20 @@ class Engine {
       GST_CUDA(cudaMemcpyAsync(d_list_, h_list_, sizeof(int) * wit.size(), cudaMemcpyHostToDevice, stream_));
       k_witness<<<(int)wit.size(), 256, 0, stream_>>>(d_slots_, d_list_, (int)wit.size(), g);
       GST_CUDA(cudaGetLastError());
+      prof_.kernel_launches += 1;
+      prof_.h2d_bytes += sizeof(int) * wit.size();
     }
     for (int t : fin) {
       auto r = slot_req_[t];
       GST_CUDA(cudaMemcpyAsync(h_slot_, d_slots_ + t, sizeof(Slot), cudaMemcpyDeviceToHost, stream_));
       GST_CUDA(cudaStreamSynchronize(stream_));
+      prof_.d2h_bytes += sizeof(Slot);
       Slot q = *h_slot_;
       gst_result& res = r->result;
       std::memset(&res, 0, sizeof res);
       res.root = -1;
       float ms = 0;
-      cudaEventElapsedTime(&ms, r->t0, t1);
+      GST_CUDA(cudaEventElapsedTime(&ms, r->t0, t1));
       res.stats.device_ms = ms;
       res.stats.rounds = q.rounds;
       res.stats.frontier = (int64_t)q.st_frontier;
@@ -633,6 +679,7 @@ class Engine {
         const int ne = q.nwedges;
         std::vector<int32_t> e(3 * (size_t)ne);
         if (ne) GST_CUDA(cudaMemcpy(e.data(), q.wedges, sizeof(int32_t) * 3 * ne, cudaMemcpyDeviceToHost));
+        prof_.d2h_bytes += sizeof(int32_t) * 3 * ne;
         // the derivation may list an edge twice; report each edge once
         std::set<std::pair<int, int>> seen;
         std::vector<int32_t> uniq;
@@ -656,6 +703,7 @@ class Engine {
       k_reset<<<num_sms_ * 2, 256, 0, stream_>>>(d_slots_, t, g);
       k_free_slot<<<1, 1, 0, stream_>>>(d_slots_, t);
       GST_CUDA(cudaGetLastError());
+      prof_.kernel_launches += 2;
       cache_[slot_slab_[t].shape].push_back(slot_slab_[t]);
       slot_busy_[t] = 0;
       slot_req_[t] = nullptr;
@@ -696,6 +744,10 @@ class Engine {
   int nslots_hw_ = 0;
   cudaGraphExec_t graph_exec_ = nullptr;
   int graph_rounds_ = 0, graph_slots_ = 0;
+  bool profile_ = false;
+  std::vector<cudaEvent_t> ev_prof_;
+  cudaEvent_t ev_run0_ = nullptr, ev_run1_ = nullptr;
+  gst_profile prof_{};
 };
 
 }  // namespace gst
@@ -749,6 +801,12 @@ gst_status gst_engine_load_graph(gst_engine* e, int64_t V, const int64_t* rowptr
 gst_status gst_engine_load_groups(gst_engine* e, int64_t n, const int64_t* ptr, const int32_t* members) {
   if (!e) return gst::fail(GST_E_INVALID, "null engine");
   return e->eng.load_groups(n, ptr, members);
+}
+
+gst_status gst_engine_profile(gst_engine* e, gst_profile* out) {
+  if (!e || !out) return gst::fail(GST_E_INVALID, "gst_engine_profile: null argument");
+  *out = e->eng.profile();
+  return GST_OK;
 }
 
 void gst_result_free(gst_result* r) {

@@ -34,7 +34,7 @@ EXPORTS = [
     "gst_read_queries", "gst_csr_free", "gst_groups_free", "gst_queries_free",
     "gst_engine_create", "gst_engine_destroy", "gst_engine_load_graph", "gst_engine_load_groups",
     "gst_result_free", "gst_solve", "gst_solve_batch", "gst_server_start", "gst_server_submit",
-    "gst_server_wait", "gst_server_stop",
+    "gst_server_wait", "gst_server_stop", "gst_engine_profile",
 ]
 
 
@@ -62,7 +62,15 @@ class _Queries(ctypes.Structure):
 class _Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("arena_fraction", ctypes.c_double),
                 ("arena_bytes", ctypes.c_int64), ("max_slots", ctypes.c_int),
-                ("rounds_per_poll", ctypes.c_int), ("max_rounds", ctypes.c_int)]
+                ("rounds_per_poll", ctypes.c_int), ("max_rounds", ctypes.c_int),
+                ("profile", ctypes.c_int)]
+
+
+class _Profile(ctypes.Structure):
+    _fields_ = [("run_ms", ctypes.c_double), ("grow_ms", ctypes.c_double),
+                ("grow_launches", ctypes.c_int64), ("merge_ms", ctypes.c_double),
+                ("merge_launches", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
+                ("rounds", ctypes.c_int64), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64)]
 
 
 class _Stats(ctypes.Structure):
@@ -111,6 +119,8 @@ def load_library() -> ctypes.CDLL:
     lib.gst_server_start.argtypes = [P, ctypes.POINTER(P)]
     lib.gst_server_submit.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]
     lib.gst_server_wait.argtypes = [P, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(_Result)]
+    lib.gst_engine_profile.argtypes = [P, ctypes.POINTER(_Profile)]
+    lib.gst_engine_profile.restype = ctypes.c_int
     lib.gst_server_stop.argtypes = [P]
     lib.gst_server_stop.restype = None
     for name in ("gst_read_input_graph", "gst_read_binary_csr", "gst_read_groups", "gst_read_queries",
@@ -218,9 +228,11 @@ class Engine:
     """One engine per device: graph + groups resident in HBM, arena for tables."""
 
     def __init__(self, device: int = 0, arena_fraction: float = 0.0, arena_bytes: int = 0,
-                 max_slots: int = 0, rounds_per_poll: int = 0, max_rounds: int = 0):
+                 max_slots: int = 0, rounds_per_poll: int = 0, max_rounds: int = 0,
+                 profile: bool = False):
         self._lib = load_library()
-        cfg = _Config(device, arena_fraction, arena_bytes, max_slots, rounds_per_poll, max_rounds)
+        cfg = _Config(device, arena_fraction, arena_bytes, max_slots, rounds_per_poll, max_rounds,
+                      1 if profile else 0)
         h = ctypes.c_void_p()
         _check(self._lib.gst_engine_create(ctypes.byref(cfg), ctypes.byref(h)), "engine_create")
         self._h = h
@@ -271,6 +283,12 @@ class Engine:
                                          None if Darr is None else Darr.ctypes.data, res,
                                          sts.ctypes.data), "solve_batch")
         return [_take_result(self._lib, res[i], int(sts[i])) for i in range(n)]
+
+    def profile(self) -> dict:
+        """Device measurements of the last solve / solve_batch call."""
+        p = _Profile()
+        _check(self._lib.gst_engine_profile(self._h, ctypes.byref(p)), "profile")
+        return {f: getattr(p, f) for f, _ in _Profile._fields_}
 
     def server(self) -> "Server":
         return Server(self)

@@ -111,6 +111,7 @@ typedef struct {
   int rounds_per_poll;     /* device rounds between host status checks (0 -> 8) */
   int max_rounds;          /* device rounds a query may take before it fails with
                               GST_E_LIMIT (0: unlimited) */
+  int profile;             /* 1: time the grow and merge kernels with CUDA events */
 } gst_engine_config;
 
 gst_status gst_engine_create(const gst_engine_config* cfg, gst_engine** out);
@@ -161,6 +162,24 @@ gst_status gst_solve(gst_engine* e, const int32_t* group_ids, int k, int D, gst_
  * counterpart: the reference solves one query per call. */
 gst_status gst_solve_batch(gst_engine* e, int64_t n, const int64_t* ptr, const int32_t* ids,
                            const int32_t* D, gst_result* out, gst_status* status_out);
+
+/* Device-side measurements of the most recent gst_solve / gst_solve_batch
+ * call.  run_ms spans the call on the engine's stream (CUDA events); the
+ * kernel times are filled when the engine was created with profile = 1.
+ * No reference counterpart (the reference times with host clocks). */
+typedef struct {
+  double run_ms;            /* device time of the call */
+  double grow_ms;           /* summed duration of the grow-kernel launches */
+  int64_t grow_launches;
+  double merge_ms;          /* summed duration of the merge-kernel launches */
+  int64_t merge_launches;
+  int64_t kernel_launches;  /* all engine kernel launches in the call */
+  int64_t rounds;           /* device rounds run */
+  int64_t h2d_bytes;        /* host-to-device bytes copied by the call */
+  int64_t d2h_bytes;        /* device-to-host bytes copied by the call */
+} gst_profile;
+
+gst_status gst_engine_profile(gst_engine* e, gst_profile* out);
 
 /* ---------------------------------------------------------------------------
  * Serving: continuous batching.  Requests submitted while others run are
