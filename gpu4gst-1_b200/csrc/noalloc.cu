@@ -1,0 +1,247 @@
+// gst_solve_noalloc: one query solved without allocating any memory.
+//
+// Some callers cannot allocate: code that runs while a caller-owned memory
+// pool must not grow (a serving process that reserved all HBM up front), code
+// inside allocation-free sections of a host framework, or plugin hosts that
+// forbid cudaMalloc/cudaFree after start-up.  For them this entry point takes
+// the graph and groups as device pointers the caller already owns, returns
+// the cost and root in host variables, and keeps every piece of scratch state
+// (DP table, dirty masks, frontier lists, chunk list, control blocks) in one
+// file-scope static device array of GST_NOALLOC_SCRATCH_BYTES.  It runs the
+// same round kernels as the engine, launched directly (no CUDA graph, whose
+// instantiation allocates).
+//
+// The array is part of this library's device image: every GPU that loads the
+// library holds it until the process exits.  All calls share it and it keeps
+// the previous call's contents, so each call re-initialises what must start
+// cleared; calls that overlap on the GPU (different host threads, or
+// different streams of one device) race on it and must be serialised by the
+// caller.  The first call on a device does a one-time set-up on that device
+// (symbol address lookup, subset tables, kernel attribute); make that first
+// call before any stream capture.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "status.hpp"  // gst::fail: the library's shared error text
+
+// This translation unit instantiates its own copy of the round kernels and
+// of the subset tables under a private namespace, so that the engine's
+// definitions are left untouched.
+#define gst gst_noalloc
+#include "engine_dev.cuh"
+#include "kernels.cuh"
+#undef gst
+
+namespace gst_noalloc {
+using gst::fail;
+namespace {
+
+constexpr size_t kScratchBytes = GST_NOALLOC_SCRATCH_BYTES;
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
+
+struct DeviceSetup {
+  bool done = false;
+  unsigned char* base = nullptr;  // device address of g_scratch
+};
+DeviceSetup g_setup[kMaxDevices];
+std::mutex g_setup_mu;
+
+void fill_tables(SubsetTables& t) {
+  std::memset(&t, 0, sizeof t);
+  for (int k = 1; k <= MAXK; ++k) {
+    const int W = 1 << k;
+    int pos = 0;
+    for (int s = 0; s <= k; ++s) {
+      t.loff[k][s] = (uint8_t)pos;
+      for (int S = 0; S < W; ++S)
+        if (__builtin_popcount(S) == s) {
+          t.sof[k][pos] = (uint8_t)S;
+          t.sidx[k][S] = (uint8_t)pos;
+          ++pos;
+        }
+    }
+    t.loff[k][k + 1] = (uint8_t)W;
+  }
+}
+
+gst_status setup_device(int dev, unsigned char** base) {
+  std::lock_guard<std::mutex> lk(g_setup_mu);
+  if (dev < 0 || dev >= kMaxDevices) return fail(GST_E_INVALID, "noalloc: device ordinal out of range");
+  DeviceSetup& s = g_setup[dev];
+  if (!s.done) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+    if (e != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    SubsetTables t;
+    fill_tables(t);
+    e = cudaMemcpyToSymbol(c_sub, &t, sizeof t);
+    if (e != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: subset tables: ") + cudaGetErrorString(e));
+    e = cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             MERGE_WARPS * MAXW * MAXL * (int)sizeof(int));
+    if (e != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: merge attribute: ") + cudaGetErrorString(e));
+    s.base = static_cast<unsigned char*>(p);
+    s.done = true;
+  }
+  *base = s.base;
+  return GST_OK;
+}
+
+size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace gst_noalloc
+
+extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_rowptr, const int32_t* d_adj,
+                                        int64_t n_groups, const int64_t* d_group_ptr,
+                                        const int32_t* d_group_members, const int32_t* group_ids, int k,
+                                        int D, void* stream, int64_t* cost_out, int32_t* root_out) {
+  using namespace gst_noalloc;
+  if (!d_rowptr || !d_adj || !d_group_ptr || !group_ids || !cost_out || !root_out || V <= 0 || E < 0 || k <= 0)
+    return fail(GST_E_INVALID, "noalloc: null pointer or empty input");
+  if (V > INT32_MAX || E >= (int64_t)UINT32_MAX) return fail(GST_E_UNSUPPORTED, "noalloc: graph too large");
+  if (D > GST_MAX_D) return fail(GST_E_UNSUPPORTED, "noalloc: D above GST_MAX_D");
+  if (D < 0) D = -1;
+  int32_t groups[MAXK];
+  int kk = 0;
+  for (int i = 0; i < k; ++i) {
+    if (group_ids[i] < 0 || group_ids[i] >= n_groups) return fail(GST_E_INVALID, "noalloc: group id out of range");
+    bool dup = false;
+    for (int j = 0; j < kk; ++j) dup |= groups[j] == group_ids[i];
+    if (dup) continue;
+    if (kk == MAXK) return fail(GST_E_UNSUPPORTED, "noalloc: more than GST_MAX_K distinct groups");
+    groups[kk++] = group_ids[i];
+  }
+  *cost_out = GST_REF_INF;
+  *root_out = -1;
+  int dev = 0;
+  cudaError_t ce = cudaGetDevice(&dev);
+  if (ce != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(ce));
+  unsigned char* base = nullptr;
+  gst_status st = setup_device(dev, &base);
+  if (st != GST_OK) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+  // group sizes (host copies of two offsets per queried group)
+  for (int i = 0; i < kk; ++i) {
+    int64_t b[2];
+    ce = cudaMemcpyAsync(b, d_group_ptr + groups[i], sizeof b, cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(ce));
+    if (b[1] == b[0]) return GST_OK;  // an empty group: infeasible
+  }
+  if (kk == 1) {  // one group: any member is a tree of cost 0
+    int32_t m = 0;
+    int64_t b = 0;
+    ce = cudaMemcpyAsync(&b, d_group_ptr + groups[0], sizeof b, cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&m, d_group_members + b, sizeof m, cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(ce));
+    *cost_out = 0;
+    *root_out = m;
+    return GST_OK;
+  }
+
+  // carve the scratch array
+  const size_t W = (size_t)1 << kk, L = D < 0 ? 1 : (size_t)D + 1, nq = D < 0 ? 2 : L;
+  const size_t chunk_cap = (size_t)V + (size_t)E / 32 + 64;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off += up256(bytes); return o; };
+  const size_t o_slot = take(sizeof(Slot));
+  const size_t o_plan = take(sizeof(Plan));
+  const size_t o_status = take(sizeof(SlotStatus));
+  const size_t o_table = take((size_t)V * W * L * 4);
+  const size_t o_mask = take(L * (size_t)V * 8);
+  const size_t o_queue = take(nq * (size_t)V * 4);
+  const size_t o_touched = take((size_t)V * 4);
+  const size_t o_tflag = take((size_t)V * 4);
+  const size_t o_chunks = take(chunk_cap * sizeof(Chunk));
+  const size_t o_lbtab = take((size_t)kk * kk * W * 4 + (size_t)kk * W * 4);
+  if (off > kScratchBytes)
+    return fail(GST_E_NOMEM, "noalloc: query needs " + std::to_string(off >> 20) + " MiB of scratch, above the " +
+                                 std::to_string(kScratchBytes >> 20) + " MiB static maximum");
+  Slot* d_slot = reinterpret_cast<Slot*>(base + o_slot);
+  Plan* d_plan = reinterpret_cast<Plan*>(base + o_plan);
+  SlotStatus* d_status = reinterpret_cast<SlotStatus*>(base + o_status);
+
+  Slot q;
+  std::memset(&q, 0, sizeof q);
+  q.table = reinterpret_cast<int32_t*>(base + o_table);
+  q.mask = reinterpret_cast<unsigned long long*>(base + o_mask);
+  q.queue = reinterpret_cast<uint32_t*>(base + o_queue);
+  q.touched = reinterpret_cast<uint32_t*>(base + o_touched);
+  q.tflag = reinterpret_cast<uint32_t*>(base + o_tflag);
+  q.chunks = reinterpret_cast<Chunk*>(base + o_chunks);
+  q.lbtab = reinterpret_cast<int32_t*>(base + o_lbtab);
+  q.wstack = nullptr;
+  q.wedges = nullptr;
+  q.chunk_cap = (long long)chunk_cap;
+  q.wcap = 0;
+  q.k = kk;
+  q.W = (int)W;
+  q.L = (int)L;
+  q.D = D;
+  for (int i = 0; i < kk; ++i) q.groups[i] = groups[i];
+  q.phase = PH_ACTIVE;
+  q.action = A_INIT;
+  q.s = 1;
+  q.cur = 1;
+  q.best = INF;
+  q.R1 = INF / 2;
+  q.answer = ~0ull;
+
+  // what must start cleared: the table (INF), dirty masks, touched flags, plan
+  ce = cudaMemsetAsync(base + o_table, 0x3f, (size_t)V * W * L * 4, s);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_mask, 0, L * (size_t)V * 8, s);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_tflag, 0, (size_t)V * 4, s);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(d_plan, 0, sizeof(Plan), s);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_slot, &q, sizeof q, cudaMemcpyHostToDevice, s);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);  // q lives on this stack frame
+  if (ce != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(ce));
+
+  Graph g;
+  g.rowptr = reinterpret_cast<const long long*>(d_rowptr);
+  g.adj = reinterpret_cast<const int2*>(d_adj);
+  g.gptr = reinterpret_cast<const long long*>(d_group_ptr);
+  g.gmem = d_group_members;
+  g.V = V;
+  g.E = E;
+  g.G = n_groups;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = nsm * 4;
+  k_init_seeds<<<64, 256, 0, s>>>(d_slot, 0, g);
+  k_init_base<<<64, 256, 0, s>>>(d_slot, 0, g);
+  const long long max_rounds = 4ll * V * (long long)L + 1000;  // far above any DP's need
+  SlotStatus hs;
+  long long rounds = 0;
+  for (;;) {
+    for (int r = 0; r < 8; ++r) {
+      k_ctl_a<<<1, MAXSLOTS, 0, s>>>(d_slot, 1, d_plan, d_status);
+      k_lbprep<<<1, 256, 0, s>>>(d_slot, d_plan, g);
+      k_merge<<<grid, MERGE_WARPS * 32, MERGE_WARPS * MAXW * MAXL * sizeof(int), s>>>(d_slot, d_plan, g);
+      k_prep<<<grid, 256, 0, s>>>(d_slot, d_plan, g);
+      k_ctl_b<<<1, MAXSLOTS, 0, s>>>(d_slot, d_plan);
+      k_grow<<<grid, GROW_WARPS * 32, 0, s>>>(d_slot, d_plan, g);
+    }
+    rounds += 8;
+    k_publish<<<1, 32, 0, s>>>(d_slot, 1, d_status);
+    ce = cudaGetLastError();
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&hs, d_status, sizeof hs, cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(ce));
+    if (hs.phase == PH_DONE || hs.phase == PH_ERROR) break;
+    if (rounds > max_rounds) return fail(GST_E_LIMIT, "noalloc: round limit exceeded");
+  }
+  if (hs.phase == PH_ERROR || hs.err != ERR_NONE) return fail(GST_E_LIMIT, "noalloc: device-side bound hit");
+  if ((hs.answer >> 32) < (unsigned long long)INF) {
+    *cost_out = (int64_t)(hs.answer >> 32);
+    *root_out = (int32_t)(hs.answer & 0xffffffffu);
+  }
+  return GST_OK;
+}

@@ -34,7 +34,7 @@ EXPORTS = [
     "gst_read_queries", "gst_csr_free", "gst_groups_free", "gst_queries_free",
     "gst_engine_create", "gst_engine_destroy", "gst_engine_load_graph", "gst_engine_load_groups",
     "gst_result_free", "gst_solve", "gst_solve_batch", "gst_server_start", "gst_server_submit",
-    "gst_server_wait", "gst_server_stop", "gst_engine_profile",
+    "gst_server_wait", "gst_server_stop", "gst_engine_profile", "gst_solve_noalloc",
 ]
 
 
@@ -119,6 +119,10 @@ def load_library() -> ctypes.CDLL:
     lib.gst_server_start.argtypes = [P, ctypes.POINTER(P)]
     lib.gst_server_submit.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]
     lib.gst_server_wait.argtypes = [P, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(_Result)]
+    lib.gst_solve_noalloc.argtypes = [ctypes.c_int64, ctypes.c_int64, P, P, ctypes.c_int64, P, P, P,
+                                      ctypes.c_int, ctypes.c_int, P, ctypes.POINTER(ctypes.c_int64),
+                                      ctypes.POINTER(ctypes.c_int32)]
+    lib.gst_solve_noalloc.restype = ctypes.c_int
     lib.gst_engine_profile.argtypes = [P, ctypes.POINTER(_Profile)]
     lib.gst_engine_profile.restype = ctypes.c_int
     lib.gst_server_stop.argtypes = [P]

@@ -182,6 +182,33 @@ typedef struct {
 gst_status gst_engine_profile(gst_engine* e, gst_profile* out);
 
 /* ---------------------------------------------------------------------------
+ * Allocation-free solve.  No counterpart in the reference.
+ * ------------------------------------------------------------------------- */
+
+#define GST_NOALLOC_SCRATCH_BYTES (64ull << 20) /* static device scratch: 64 MiB */
+
+/* One query (plain, D < 0, or diameter-bounded) for callers that cannot
+ * allocate memory: processes that reserved all device memory up front, code
+ * running in allocation-free sections, plugin hosts that forbid cudaMalloc
+ * after start-up.  Nothing is allocated: the caller passes the graph and the
+ * groups as device pointers it owns (d_adj holds E (neighbour, weight) int32
+ * pairs, interleaved; d_rowptr V+1 int64 offsets; groups as int64 offsets and
+ * int32 members), the queried group ids in host memory, and receives the
+ * cost (GST_REF_INF when infeasible) and the root vertex in host variables.
+ * All scratch lives in a file-scope static device array of
+ * GST_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit; a query whose scratch would exceed it fails with GST_E_NOMEM.  Calls
+ * share that array, so calls that overlap on the GPU race and must be
+ * serialised by the caller.  The first call on a device performs a one-time
+ * set-up on it and should come before any stream capture.  `stream` is a
+ * cudaStream_t (NULL: the legacy default stream); the call returns after the
+ * stream has finished the query. */
+gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_rowptr, const int32_t* d_adj,
+                             int64_t n_groups, const int64_t* d_group_ptr,
+                             const int32_t* d_group_members, const int32_t* group_ids, int k,
+                             int D, void* stream, int64_t* cost_out, int32_t* root_out);
+
+/* ---------------------------------------------------------------------------
  * Serving: continuous batching.  Requests submitted while others run are
  * admitted as slots and arena memory free up; their device work overlaps.
  * No reference counterpart.
