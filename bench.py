@@ -226,6 +226,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--single", type=int, default=30, help="queries timed one per call")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--queries", type=int, default=0, help="queries per step (0: the workload's count)")
+    ap.add_argument("--arena-gb", type=float, default=0.0, help="device arena size (0: 85%% of free memory)")
+    ap.add_argument("--max-slots", type=int, default=0, help="queries resident at once (0: engine default)")
+    ap.add_argument("--rounds-per-poll", type=int, default=0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -247,9 +251,12 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     wl = make_workload(args.workload, rank)
+    if args.queries > 0:
+        wl.queries = wl.queries[: args.queries]
     queries = [q for q, _ in wl.queries]
     Ds = [D for _, D in wl.queries]
-    eng = gst_b200.Engine(device=local, profile=True)
+    eng = gst_b200.Engine(device=local, profile=True, arena_bytes=int(args.arena_gb * (1 << 30)),
+                          max_slots=args.max_slots, rounds_per_poll=args.rounds_per_poll)
     eng.load_graph(wl.graph.rowptr, wl.graph.col, wl.graph.w)
     eng.load_groups(wl.groups.ptr, wl.groups.mem)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")

@@ -147,7 +147,7 @@ class Engine {
     gst_engine_config c{};
     if (cfg) c = *cfg;
     device_ = c.device;
-    max_slots_ = c.max_slots > 0 ? std::min(c.max_slots, MAXSLOTS) : 256;
+    max_slots_ = c.max_slots > 0 ? std::min(c.max_slots, MAXSLOTS) : MAXSLOTS;
     max_rounds_override_ = c.max_rounds > 0 ? c.max_rounds : 0;
     profile_ = c.profile != 0;
     rounds_per_poll_ = c.rounds_per_poll > 0 ? c.rounds_per_poll : 8;
@@ -172,8 +172,6 @@ class Engine {
     GST_CUDA(cudaMalloc(&d_list_, sizeof(int) * MAXSLOTS));
     GST_CUDA(cudaMallocHost(&h_list_, sizeof(int) * MAXSLOTS));
     GST_CUDA(cudaMallocHost(&h_slot_, sizeof(Slot)));
-    GST_CUDA(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  MERGE_WARPS * MAXW * MAXL * (int)sizeof(int)));
     size_t fr = 0, tot = 0;
     GST_CUDA(cudaMemGetInfo(&fr, &tot));
     arena_request_ = c.arena_bytes > 0 ? (size_t)c.arena_bytes
@@ -572,7 +570,7 @@ class Engine {
     k_ctl_a<<<1, MAXSLOTS, 0, st>>>(d_slots_, max_slots_, d_plan_, d_status_);
     k_lbprep<<<std::min(max_slots_, 256), 256, 0, st>>>(d_slots_, d_plan_, g);
     if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 0], st, cudaEventRecordExternal);
-    k_merge<<<grid, MERGE_WARPS * 32, MERGE_WARPS * MAXW * MAXL * sizeof(int), st>>>(d_slots_, d_plan_, g);
+    k_merge<<<grid, MERGE_THREADS, 0, st>>>(d_slots_, d_plan_, g);
     if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 1], st, cudaEventRecordExternal);
     k_prep<<<grid, 256, 0, st>>>(d_slots_, d_plan_, g);
     k_ctl_b<<<1, MAXSLOTS, 0, st>>>(d_slots_, d_plan_);

@@ -196,7 +196,8 @@ __global__ void k_ctl_a(Slot* slots, int nslots, Plan* plan, SlotStatus* status)
               act = (q.s == q.k) ? A_MERGEFULL : A_MERGE;
             }
           }
-          if (act == A_MERGE || act == A_MERGEFULL) n_merge = q.ntouched;
+          if (act == A_MERGE || act == A_MERGEFULL)  // one item per (touched vertex, set of the layer)
+            n_merge = (long long)q.ntouched * (c_sub.loff[q.k][q.s + 1] - c_sub.loff[q.k][q.s]);
           if (act == A_GROW) n_prep = hop ? q.qcount[q.d] : q.qcount[q.cur];
         }
       }
@@ -338,93 +339,202 @@ __global__ void k_lbprep(Slot* slots, const Plan* plan, Graph g) {
 }
 
 // ---------------------------------------------------------------------------
-// Merge: subset join of layer s at every touched vertex (one warp per vertex,
-// the vertex's row staged in shared memory).
+// Merge: subset join of layer s.  One thread per (touched vertex, set of the
+// layer); the vertex's row is read through L1 (the threads of one vertex are
+// adjacent, so its row is fetched once).  LT is the compile-time label count
+// (1 = plain); 0 handles any count.
 // ---------------------------------------------------------------------------
-constexpr int MERGE_WARPS = 8;
+constexpr int MERGE_THREADS = 256;
 
-__global__ void __launch_bounds__(MERGE_WARPS * 32)
-k_merge(Slot* slots, const Plan* plan, Graph g) {
-  extern __shared__ int s_rows[];  // MERGE_WARPS x (MAXW * MAXL)
+// Segmented (by key, keys contiguous in lane order) reductions; the first lane
+// of each segment ends with the result.
+__device__ __forceinline__ unsigned long long seg_min_u64(unsigned long long v, unsigned long long key) {
   const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  int* srow = s_rows + wib * (MAXW * MAXL);
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long ov = __shfl_down_sync(0xffffffffu, v, o);
+    const unsigned long long ok = __shfl_down_sync(0xffffffffu, key, o);
+    if (lane + o < 32 && ok == key && ov < v) v = ov;
+  }
+  return v;
+}
+__device__ __forceinline__ unsigned long long seg_or_u64(unsigned long long v, unsigned long long key) {
+  const int lane = threadIdx.x & 31;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long ov = __shfl_down_sync(0xffffffffu, v, o);
+    const unsigned long long ok = __shfl_down_sync(0xffffffffu, key, o);
+    if (lane + o < 32 && ok == key) v |= ov;
+  }
+  return v;
+}
+__device__ __forceinline__ unsigned long long seg_add_u64(unsigned long long v, unsigned long long key) {
+  const int lane = threadIdx.x & 31;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long ov = __shfl_down_sync(0xffffffffu, v, o);
+    const unsigned long long ok = __shfl_down_sync(0xffffffffu, key, o);
+    if (lane + o < 32 && ok == key) v += ov;
+  }
+  return v;
+}
+__device__ __forceinline__ bool seg_head(unsigned long long key) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long pk = __shfl_up_sync(0xffffffffu, key, 1);
+  return lane == 0 || pk != key;
+}
+
+// Merged costs M[0..L) (prefix minima over labels) of set S at a vertex row.
+template <int LT>
+__device__ __forceinline__ void merge_costs(const int32_t* row, int k, int S, int Lrt, int D, int* M) {
+  const int L = LT > 0 ? LT : Lrt;
+  const int base = c_sub.sidx[k][S] * L;
+  {
+    int m = INF;
+#pragma unroll
+    for (int l = 0; l < (LT > 0 ? LT : MAXL); ++l) {
+      if (LT == 0 && l >= L) break;
+      m = imin(m, row[base + l]);
+      M[l] = m;
+    }
+  }
+  for (int S1 = (S - 1) & S; S1 > 0; S1 = (S1 - 1) & S) {
+    const int S2 = S ^ S1;
+    if (S1 < S2) continue;
+    const int i1 = c_sub.sidx[k][S1] * L, i2 = c_sub.sidx[k][S2] * L;
+    if (LT == 1) {
+      M[0] = imin(M[0], row[i1] + row[i2]);
+    } else {
+      int a[LT > 0 ? LT : MAXL], b[LT > 0 ? LT : MAXL];
+      int ma = INF, mb = INF;
+#pragma unroll
+      for (int l = 0; l < (LT > 0 ? LT : MAXL); ++l) {
+        if (LT == 0 && l >= L) break;
+        ma = imin(ma, row[i1 + l]);
+        mb = imin(mb, row[i2 + l]);
+        a[l] = ma;
+        b[l] = mb;
+      }
+#pragma unroll
+      for (int l = 0; l < (LT > 0 ? LT : MAXL); ++l) {
+        if (LT == 0 && l >= L) break;
+        const int m2 = imin(l, D - l);
+        M[l] = imin(M[l], imin(a[l] + b[m2], a[m2] + b[l]));
+      }
+    }
+  }
+#pragma unroll
+  for (int l = 1; l < (LT > 0 ? LT : MAXL); ++l) {
+    if (LT == 0 && l >= L) break;
+    M[l] = imin(M[l], M[l - 1]);
+  }
+}
+
+template <int LT>
+__device__ __forceinline__ void merge_item(Slot& q, int t, uint32_t v, int r, Graph& g,
+                                           unsigned long long* ans, unsigned long long* dirty0) {
+  const int k = q.k, W = q.W, L = LT > 0 ? LT : q.L, rowlen = W * L, D = q.D, s = q.s;
+  const bool hop = D >= 0;
+  const int lo = c_sub.loff[k][s];
+  const int S = c_sub.sof[k][lo + r];
+  int32_t* row = q.table + (long long)v * rowlen;
+  int M[LT > 0 ? LT : MAXL];
+  merge_costs<LT>(row, k, S, L, D, M);
+  if (s == k) {
+    const int a = M[L - 1];
+    if (a < INF) *ans = ((unsigned long long)(unsigned)a << 32) | (unsigned long long)v;
+    return;
+  }
+  const int best = *(volatile int*)&q.best;
+  int dist[MAXK];
+  for (int i = 0; i < k; ++i) {
+    int dm = INF;
+    for (int l = 0; l < L; ++l) dm = imin(dm, row[(1 + i) * L + l]);
+    dist[i] = clip_dist(dm, q.R1);
+  }
+  const int lbv = lower_bound(dist, k, W, S, q.lbtab);
+  for (int l = 0; l < L; ++l) {
+    const int val = M[l];
+    if (val >= INF) continue;
+    if (l > 0 && val >= M[l - 1]) continue;     // no better than a smaller label
+    if ((long long)val + lbv > best) continue;  // cannot be part of an optimum
+    const long long idx = (long long)(lo + r) * L + l;
+    if (val < row[idx]) row[idx] = val;
+    // star upper bound: the cheapest path to every missing group
+    long long ub = val;
+    const int hl = hop ? imin(l, D - l) : 0;
+    for (int i = 0; i < k && ub < INF; ++i)
+      if (!((S >> i) & 1)) {
+        int dm = INF;
+        for (int x = 0; x <= hl; ++x) dm = imin(dm, row[(1 + i) * L + x]);
+        ub += dm;
+      }
+    if (ub < best) atomicMin(&q.best, (int)ub);
+    if (2LL * val <= best && (!hop || l < D)) {
+      if (!hop) *dirty0 |= 1ull << r;  // plain: aggregated per vertex by the caller
+      else mark_dirty(q, g.V, v, r, l, l);
+    }
+  }
+  (void)t;
+}
+
+__global__ void __launch_bounds__(MERGE_THREADS)
+k_merge(Slot* slots, const Plan* plan, Graph g) {
+  __shared__ long long s_off[MAXSLOTS + 1];
+  __shared__ int s_slot[MAXSLOTS];
   const int nm = plan->n_merge;
   if (nm == 0) return;
-  const long long total = plan->merge_off[nm];
-  const long long nwarps = (long long)gridDim.x * MERGE_WARPS;
-  for (long long gi = blockIdx.x * (long long)MERGE_WARPS + wib; gi < total; gi += nwarps) {
-    const int j = seg_search(plan->merge_off, nm, gi);
-    Slot& q = slots[plan->merge_slots[j]];
-    const uint32_t v = q.touched[gi - plan->merge_off[j]];
-    const int k = q.k, W = q.W, L = q.L, rowlen = W * L, D = q.D, s = q.s;
-    const bool hop = D >= 0;
-    const int best = *(volatile int*)&q.best;
-    const int R1 = q.R1;
-    int32_t* vrow = q.table + (long long)v * rowlen;
-    // stage the row; raw values kept in registers for the layer's own sets
-    for (int x = lane; x < rowlen; x += 32) srow[x] = vrow[x];
-    __syncwarp();
-    if (hop) {  // prefix minima over labels
-      for (int x = lane; x < W; x += 32) {
-        int m = INF;
-        for (int l = 0; l < L; ++l) {
-          m = imin(m, srow[x * L + l]);
-          srow[x * L + l] = m;
-        }
+  for (int x = threadIdx.x; x <= nm; x += blockDim.x) s_off[x] = plan->merge_off[x];
+  for (int x = threadIdx.x; x < nm; x += blockDim.x) s_slot[x] = plan->merge_slots[x];
+  __syncthreads();
+  const long long total = s_off[nm];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  // every lane of a warp iterates the same number of times (shuffles below)
+  const long long span = (total + 31) & ~31ll;
+  for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < span; gi += stride) {
+    unsigned long long ans = ~0ull, dirty = 0, key = ~0ull;
+    int t = -1;
+    uint32_t v = 0;
+    unsigned long long nsplit = 0;
+    if (gi < total) {
+      const int j = seg_search(s_off, nm, gi);
+      t = s_slot[j];
+      Slot& q = slots[t];
+      const int k = q.k, s = q.s;
+      const int lo = c_sub.loff[k][s], nS = c_sub.loff[k][s + 1] - lo;
+      const long long local = gi - s_off[j];
+      const int vi = (int)(local / nS), r = (int)(local % nS);
+      v = q.touched[vi];
+      key = ((unsigned long long)(unsigned)t << 32) | (unsigned)vi;
+      switch (q.L) {
+        case 1: merge_item<1>(q, t, v, r, g, &ans, &dirty); break;
+        case 3: merge_item<3>(q, t, v, r, g, &ans, &dirty); break;
+        case 4: merge_item<4>(q, t, v, r, g, &ans, &dirty); break;
+        case 5: merge_item<5>(q, t, v, r, g, &ans, &dirty); break;
+        case 6: merge_item<6>(q, t, v, r, g, &ans, &dirty); break;
+        default: merge_item<0>(q, t, v, r, g, &ans, &dirty); break;
       }
-      __syncwarp();
-    }
-    int dist[MAXK];
-    for (int i = 0; i < k; ++i) dist[i] = clip_dist(srow[(1 + i) * L + (L - 1)], R1);
-    const int lo = c_sub.loff[k][s], nS = c_sub.loff[k][s + 1] - lo;
-    unsigned long long nmerge = 0;
-    for (int r = lane; r < nS; r += 32) {
       const int S = c_sub.sof[k][lo + r];
-      int M[MAXL];
-      for (int l = 0; l < L; ++l) M[l] = srow[(lo + r) * L + l];
-      for (int S1 = (S - 1) & S; S1 > 0; S1 = (S1 - 1) & S) {
-        const int S2 = S ^ S1;
-        if (S1 < S2) continue;
-        const int i1 = c_sub.sidx[k][S1] * L, i2 = c_sub.sidx[k][S2] * L;
-        ++nmerge;
-        if (!hop) {
-          M[0] = imin(M[0], srow[i1] + srow[i2]);
-        } else {
-          for (int l = 0; l < L; ++l) {
-            const int m2 = imin(l, D - l);
-            const int c = imin(srow[i1 + l] + srow[i2 + m2], srow[i1 + m2] + srow[i2 + l]);
-            M[l] = imin(M[l], c);
-          }
-        }
-      }
-      for (int l = 1; l < L; ++l) M[l] = imin(M[l], M[l - 1]);
-      if (s == k) {
-        const int ans = M[L - 1];
-        if (ans < INF)
-          atomicMin(&q.answer, ((unsigned long long)(unsigned)ans << 32) | (unsigned long long)v);
-        continue;
-      }
-      const int lbv = lower_bound(dist, k, W, S, q.lbtab);
-      for (int l = 0; l < L; ++l) {
-        const int val = M[l];
-        if (val >= INF) continue;
-        if (l > 0 && val >= M[l - 1]) continue;      // no better than a smaller label
-        if ((long long)val + lbv > best) continue;   // cannot be part of an optimum
-        const long long idx = (long long)(lo + r) * L + l;
-        if (val < vrow[idx]) vrow[idx] = val;
-        // star upper bound: join the cheapest path to every missing group
-        long long ub = val;
-        const int hl = hop ? imin(l, D - l) : 0;
-        for (int i = 0; i < k && ub < INF; ++i)
-          if (!((S >> i) & 1)) ub += srow[(1 + i) * L + hl];
-        if (ub < best) atomicMin(&q.best, (int)ub);
-        if (2LL * val <= best && (!hop || l < D)) mark_dirty(q, g.V, v, r, hop ? l : 0, hop ? l : (q.cur ^ 1));
+      nsplit = (1ull << (__popc(S) - 1)) - 1;
+    }
+    // answers: one atomic per (warp, slot).  The segment reductions and heads
+    // use full-warp shuffles, so every lane evaluates them unconditionally.
+    const unsigned long long skey = t < 0 ? ~0ull : (unsigned long long)(unsigned)t;
+    const unsigned long long amin = seg_min_u64(ans, skey);
+    const bool shead = seg_head(skey);
+    const bool vhead = seg_head(key);
+    if (t >= 0 && shead && amin != ~0ull) atomicMin(&slots[t].answer, amin);
+    // plain dirty bits: one atomicOr (and at most one enqueue) per (warp, vertex)
+    const unsigned long long dor = seg_or_u64(dirty, key);
+    if (t >= 0 && vhead && dor) {
+      Slot& q = slots[t];
+      const unsigned long long om = atomicOr(&q.mask[v], dor);
+      if (om == 0ull) {
+        const int qi = q.cur ^ 1;
+        const int pos = atomicAdd(&q.qcount[qi], 1);
+        if (pos < g.V) q.queue[(long long)qi * g.V + pos] = v;
+        else q.err = ERR_QUEUE_CAP;
       }
     }
-    for (int o = 16; o; o >>= 1) nmerge += __shfl_down_sync(0xffffffffu, nmerge, o);
-    if (lane == 0 && nmerge) atomicAdd(&q.st_merges, nmerge);
-    __syncwarp();
+    const unsigned long long ns = seg_add_u64(nsplit, skey);
+    if (t >= 0 && shead && ns) atomicAdd(&slots[t].st_merges, ns);
   }
 }
 
@@ -444,7 +554,18 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
     const int lvl = hop ? q.d : 0;
     const int qi = hop ? q.d : q.cur;
     const uint32_t v = q.queue[(long long)qi * g.V + (gi - plan->prep_off[j])];
-    const unsigned long long m = atomicExch(&q.mask[(long long)lvl * g.V + v], 0ull);
+    unsigned long long m = atomicExch(&q.mask[(long long)lvl * g.V + v], 0ull);
+    if (m == 0ull) continue;
+    {  // keep the sets whose cost is still a valid grow source (2 * cost <= best)
+      const int best = *(volatile int*)&q.best;
+      const int k = q.k, L = q.L, lo = c_sub.loff[k][q.s];
+      const int32_t* src = q.table + (long long)v * q.W * L;
+      for (unsigned long long x = m; x; x &= x - 1) {
+        const int r = __ffsll((long long)x) - 1;
+        const int sv = src[(lo + r) * L + lvl];
+        if (sv >= INF || 2LL * sv > best) m &= ~(1ull << r);
+      }
+    }
     if (m == 0ull) continue;
     const long long eb = g.rowptr[v], ee = g.rowptr[v + 1];
     const int nb = __popcll(m);
@@ -473,30 +594,79 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
 // evaluated for candidates that improve it.
 // ---------------------------------------------------------------------------
 constexpr int GROW_WARPS = 8;
+constexpr int GROW_UNROLL = 4;
 
-__global__ void __launch_bounds__(GROW_WARPS * 32)
+// Lower-bound test of a grow candidate (cold path: only improving candidates
+// reach it), kept out of line so the relaxation loop stays small.
+__device__ __noinline__ bool lb_prunes(const int32_t* trow, int k, int W, int L, int S, int R1,
+                                       const int32_t* lbtab, int nc, int best) {
+  int dist[MAXK];
+  for (int i = 0; i < k; ++i) {
+    int dm = INF;
+    for (int l = 0; l < L; ++l) dm = imin(dm, trow[(1 + i) * L + l]);
+    dist[i] = clip_dist(dm, R1);
+  }
+  return (long long)nc + lower_bound(dist, k, W, S, lbtab) > best;
+}
+
+// Adds a warp's relaxation counters to its slot (one atomic pair per flush).
+__device__ __forceinline__ void flush_counts(Slot& q, unsigned long long& nrel, unsigned long long& nimp) {
+  for (int o = 16; o; o >>= 1) {
+    nrel += __shfl_down_sync(0xffffffffu, nrel, o);
+    nimp += __shfl_down_sync(0xffffffffu, nimp, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (nrel) atomicAdd(&q.st_relax, nrel);
+    if (nimp) atomicAdd(&q.st_improve, nimp);
+  }
+  nrel = 0;
+  nimp = 0;
+}
+
+// Star upper bound at a vertex that just improved a singleton entry.
+__device__ __noinline__ void star_bound(Slot& q, const int32_t* trow, int k, int L, int hl) {
+  long long ub = 0;
+  for (int i = 0; i < k && ub < INF; ++i) {
+    int dm = INF;
+    for (int l = 0; l <= hl; ++l) dm = imin(dm, trow[(1 + i) * L + l]);
+    ub += dm;
+  }
+  if (ub < *(volatile int*)&q.best) atomicMin(&q.best, (int)ub);
+}
+
+__global__ void __launch_bounds__(GROW_WARPS * 32, 2)
 k_grow(Slot* slots, const Plan* plan, Graph g) {
+  __shared__ long long s_off[MAXSLOTS + 1];
+  __shared__ int s_slot[MAXSLOTS];
   __shared__ int s_r[GROW_WARPS][64];
   __shared__ int s_sv[GROW_WARPS][64];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int ng = plan->n_grow;
   if (ng == 0) return;
-  const long long total = plan->chunk_off[ng];
+  for (int x = threadIdx.x; x <= ng; x += blockDim.x) s_off[x] = plan->chunk_off[x];
+  for (int x = threadIdx.x; x < ng; x += blockDim.x) s_slot[x] = plan->grow_slots[x];
+  __syncthreads();
+  const long long total = s_off[ng];
   const long long nwarps = (long long)gridDim.x * GROW_WARPS;
+  unsigned long long nrel = 0, nimp = 0;  // flushed when the slot changes
+  int cur_slot = -1;
   for (long long gi = blockIdx.x * (long long)GROW_WARPS + wib; gi < total; gi += nwarps) {
-    const int j = seg_search(plan->chunk_off, ng, gi);
-    Slot& q = slots[plan->grow_slots[j]];
-    const Chunk c = q.chunks[gi - plan->chunk_off[j]];
+    const int j = seg_search(s_off, ng, gi);
+    if (s_slot[j] != cur_slot) {
+      if (cur_slot >= 0) flush_counts(slots[cur_slot], nrel, nimp);
+      cur_slot = s_slot[j];
+    }
+    Slot& q = slots[s_slot[j]];
+    const Chunk c = q.chunks[gi - s_off[j]];
     const int k = q.k, W = q.W, L = q.L, rowlen = W * L, D = q.D, s = q.s;
     const bool hop = D >= 0;
     const int d = hop ? q.d : 0;
     const int td = hop ? d + 1 : 0;
     const int best = *(volatile int*)&q.best;
-    const int R1 = q.R1;
     const int lo = c_sub.loff[k][s];
     const int32_t* src = q.table + (long long)c.v * rowlen;
-    // dirty sets whose source cost is still a valid grow source
+    // the chunk's dirty sets (filtered to valid grow sources by the prep pass)
     int nact = 0;
     for (int base = 0; base < 64; base += 32) {
       const int b = base + lane;
@@ -504,7 +674,6 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
       if ((c.mask >> b) & 1ull) {
         r = b;
         sv = src[(lo + r) * L + d];
-        if (sv >= INF || 2LL * sv > best) r = -1;
       }
       const unsigned ok = __ballot_sync(0xffffffffu, r >= 0);
       if (r >= 0) {
@@ -515,63 +684,62 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
       nact += __popc(ok);
     }
     __syncwarp();
-    unsigned long long nrel = 0, nimp = 0;
     if (nact > 0) {
-      const long long npairs = (long long)(c.ee - c.eb) * nact;
-      for (long long p = lane; p < npairs; p += 32) {
-        const long long e = c.eb + p / nact;
-        const int bi = (int)(p % nact);
-        const int2 a = __ldg(&g.adj[e]);
-        const uint32_t u = (uint32_t)a.x;
-        const int nc = s_sv[wib][bi] + a.y;
-        ++nrel;
-        if (nc >= INF) continue;
-        const int r = s_r[wib][bi];
-        int32_t* trow = q.table + (long long)u * rowlen;
-        const long long tidx = (long long)(lo + r) * L;
-        int cur = trow[tidx + td];
-        for (int l = 0; l < td; ++l) cur = imin(cur, trow[tidx + l]);
-        if (nc >= cur) continue;
-        if (s >= 2) {
-          int dist[MAXK];
-          for (int i = 0; i < k; ++i) {
-            int dm = INF;
-            for (int l = 0; l < L; ++l) dm = imin(dm, trow[(1 + i) * L + l]);
-            dist[i] = clip_dist(dm, R1);
+      const int npairs = (int)(c.ee - c.eb) * nact;
+      // pair p = (edge p / nact, set p % nact), advanced incrementally by 32;
+      // GROW_UNROLL pairs per lane are loaded before any is compared, so each
+      // lane keeps several neighbour and target reads in flight
+      const int q32 = 32 / nact, r32 = 32 % nact;
+      int e = (int)c.eb + lane / nact, bi = lane % nact;
+      for (int p = lane; p < npairs; p += 32 * GROW_UNROLL) {
+        int2 a[GROW_UNROLL];
+        int rr[GROW_UNROLL], nc[GROW_UNROLL], cur[GROW_UNROLL];
+#pragma unroll
+        for (int i = 0; i < GROW_UNROLL; ++i) {
+          nc[i] = INF;
+          rr[i] = 0;
+          if (p + 32 * i < npairs) {
+            a[i] = __ldg(&g.adj[e]);
+            rr[i] = s_r[wib][bi];
+            nc[i] = s_sv[wib][bi] + a[i].y;
+            ++nrel;
           }
-          const int S = c_sub.sof[k][lo + r];
-          if ((long long)nc + lower_bound(dist, k, W, S, q.lbtab) > best) continue;
+          e += q32;
+          bi += r32;
+          if (bi >= nact) { bi -= nact; ++e; }
         }
-        const int old = atomicMin(&trow[tidx + td], nc);
-        if (old <= nc) continue;
-        ++nimp;
-        touch(q, u);
-        if (s == 1) {  // star upper bound from a vertex that reaches every group
-          long long ub = 0;
-          const int hl = hop ? D / 2 : 0;
-          if (!hop || td <= hl) {
-            for (int i = 0; i < k && ub < INF; ++i) {
-              int dm = INF;
-              for (int l = 0; l <= hl; ++l) dm = imin(dm, trow[(1 + i) * L + l]);
-              ub += dm;
-            }
-            if (ub < best) atomicMin(&q.best, (int)ub);
+#pragma unroll
+        for (int i = 0; i < GROW_UNROLL; ++i) {
+          cur[i] = INF;
+          if (nc[i] < INF) {
+            const int32_t* trow = q.table + (long long)a[i].x * rowlen;
+            const long long tidx = (long long)(lo + rr[i]) * L;
+            int cv = trow[tidx + td];
+            for (int l = 0; l < td; ++l) cv = imin(cv, trow[tidx + l]);
+            cur[i] = cv;
           }
         }
-        if (2LL * nc <= best && (!hop || td < D))
-          mark_dirty(q, g.V, u, r, hop ? td : 0, hop ? td : (q.cur ^ 1));
+#pragma unroll
+        for (int i = 0; i < GROW_UNROLL; ++i) {
+          if (nc[i] >= cur[i]) continue;  // also skips pairs past the end (nc = INF)
+          const uint32_t u = (uint32_t)a[i].x;
+          const int r = rr[i];
+          int32_t* trow = q.table + (long long)u * rowlen;
+          const long long tidx = (long long)(lo + r) * L;
+          if (s >= 2 && lb_prunes(trow, k, W, L, c_sub.sof[k][lo + r], q.R1, q.lbtab, nc[i], best)) continue;
+          const int old = atomicMin(&trow[tidx + td], nc[i]);
+          if (old <= nc[i]) continue;
+          ++nimp;
+          touch(q, u);
+          if (s == 1 && (!hop || td <= D / 2)) star_bound(q, trow, k, L, hop ? D / 2 : 0);
+          if (2LL * nc[i] <= best && (!hop || td < D))
+            mark_dirty(q, g.V, u, r, hop ? td : 0, hop ? td : (q.cur ^ 1));
+        }
       }
-    }
-    for (int o = 16; o; o >>= 1) {
-      nrel += __shfl_down_sync(0xffffffffu, nrel, o);
-      nimp += __shfl_down_sync(0xffffffffu, nimp, o);
-    }
-    if (lane == 0) {
-      atomicAdd(&q.st_relax, nrel);
-      if (nimp) atomicAdd(&q.st_improve, nimp);
     }
     __syncwarp();
   }
+  if (cur_slot >= 0) flush_counts(slots[cur_slot], nrel, nimp);
 }
 
 // ---------------------------------------------------------------------------

@@ -17,7 +17,7 @@
 // cleared; calls that overlap on the GPU (different host threads, or
 // different streams of one device) race on it and must be serialised by the
 // caller.  The first call on a device does a one-time set-up on that device
-// (symbol address lookup, subset tables, kernel attribute); make that first
+// (symbol address lookup, subset tables); make that first
 // call before any stream capture.
 #include <cuda_runtime.h>
 
@@ -81,9 +81,6 @@ gst_status setup_device(int dev, unsigned char** base) {
     fill_tables(t);
     e = cudaMemcpyToSymbol(c_sub, &t, sizeof t);
     if (e != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: subset tables: ") + cudaGetErrorString(e));
-    e = cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             MERGE_WARPS * MAXW * MAXL * (int)sizeof(int));
-    if (e != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: merge attribute: ") + cudaGetErrorString(e));
     s.base = static_cast<unsigned char*>(p);
     s.done = true;
   }
@@ -224,7 +221,7 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
     for (int r = 0; r < 8; ++r) {
       k_ctl_a<<<1, MAXSLOTS, 0, s>>>(d_slot, 1, d_plan, d_status);
       k_lbprep<<<1, 256, 0, s>>>(d_slot, d_plan, g);
-      k_merge<<<grid, MERGE_WARPS * 32, MERGE_WARPS * MAXW * MAXL * sizeof(int), s>>>(d_slot, d_plan, g);
+      k_merge<<<grid, MERGE_THREADS, 0, s>>>(d_slot, d_plan, g);
       k_prep<<<grid, 256, 0, s>>>(d_slot, d_plan, g);
       k_ctl_b<<<1, MAXSLOTS, 0, s>>>(d_slot, d_plan);
       k_grow<<<grid, GROW_WARPS * 32, 0, s>>>(d_slot, d_plan, g);

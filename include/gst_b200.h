@@ -107,7 +107,7 @@ typedef struct {
   int device;              /* CUDA device ordinal */
   double arena_fraction;   /* share of free device memory for the arena (0 -> 0.85) */
   int64_t arena_bytes;     /* explicit arena size; overrides the fraction when > 0 */
-  int max_slots;           /* queries resident at once (0 -> 256, max 1024) */
+  int max_slots;           /* queries resident at once (0 or above 1024 -> 1024) */
   int rounds_per_poll;     /* device rounds between host status checks (0 -> 8) */
   int max_rounds;          /* device rounds a query may take before it fails with
                               GST_E_LIMIT (0: unlimited) */
