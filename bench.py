@@ -184,6 +184,86 @@ def cpu_reference_sample(wl, name: str, n_queries: int, procs: int, timeout: flo
     return len(qs) / wall, [], kind, len(ranges), len(qs), k
 
 
+def reference_gpu_sample(wl, name: str, n: int, timeout: float = 900):
+    """Runs the reference GPU program TrimCDP (built for sm_100a into
+    oracle/_ref) on the first n plain queries of the workload, one query after
+    another as the reference does.  Returns its wall time (incl. its graph
+    load), its own Relax-loop times (its `rt` column) and its costs.  A GPU
+    comparator beside the CPU baseline, not the CPU baseline."""
+    import oracle
+    from gst_b200 import datagen as dg
+    exe = oracle.ref_binary("TrimCDP")
+    if not os.path.exists(exe):
+        return None
+    d = tempfile.mkdtemp(prefix="gstrefgpu_")
+    plain = [(q, D) for q, D in wl.queries if D < 0]
+    k = sorted({len(q) for q, _ in plain})[0]
+    qs = [(q, D) for q, D in plain if len(q) == k][:n]
+    dg.write_dataset(d, name, dg.Workload(wl.graph, wl.groups, []), binary=False)
+    dg.write_queries(os.path.join(d, f"{name}{k}.csv"), qs)
+    t0 = time.time()
+    subprocess.run([exe, "2", d + "/", name, str(k), "0", str(len(qs) - 1)], check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, stdin=subprocess.DEVNULL, timeout=timeout)
+    wall = time.time() - t0
+    rt, cost = [], []
+    with open(os.path.join(d, "result", f"exp_GPU1_nonHop_{name}_T{k}_0-{len(qs) - 1}.csv")) as f:
+        next(f)
+        for line in f:
+            if line.strip():
+                p = line.split(",")
+                rt.append(float(p[2]))
+                cost.append(int(p[3]))
+    return {"queries": len(qs), "k": k, "wall_s": wall, "relax_loop_s_median": statistics.median(rt),
+            "relax_loop_s_total": sum(rt), "costs": cost}
+
+
+def run_serving(args):
+    """Poisson arrivals at --serve queries/s through the engine's serving loop
+    (continuous batching); reports per-query latency from submit to result and
+    the sustained throughput."""
+    import numpy as np
+    import gst_b200
+    wl = make_workload(args.workload, 0)
+    if args.queries > 0:
+        wl.queries = wl.queries[: args.queries]
+    eng = gst_b200.Engine(device=0, arena_bytes=int(args.arena_gb * (1 << 30)))
+    eng.load_graph(wl.graph.rowptr, wl.graph.col, wl.graph.w)
+    eng.load_groups(wl.groups.ptr, wl.groups.mem)
+    alone = eng.solve_batch([q for q, _ in wl.queries], [D for _, D in wl.queries])
+    rng = np.random.default_rng(7)
+    gaps = rng.exponential(1.0 / args.serve, size=len(wl.queries))
+    lat = [None] * len(wl.queries)
+    got = [None] * len(wl.queries)
+    with eng.server() as srv:
+        def waiter(i, ticket, t_sub):  # one waiter per request: latency = submit -> result
+            r = srv.wait(ticket)
+            lat[i] = time.perf_counter() - t_sub
+            got[i] = r.cost
+
+        ths = []
+        t0 = time.perf_counter()
+        t_next = t0
+        for i, (q, D) in enumerate(wl.queries):
+            t_next += gaps[i]
+            while time.perf_counter() < t_next:
+                time.sleep(0.0002)
+            t_sub = time.perf_counter()
+            th = threading.Thread(target=waiter, args=(i, srv.submit(q, D), t_sub))
+            th.start()
+            ths.append(th)
+        for th in ths:
+            th.join()
+        span = time.perf_counter() - t0
+    eng.close()
+    ms = np.array(lat) * 1e3
+    print(json.dumps({
+        "mode": "serving", "workload": WORKLOADS[args.workload], "arrival_rate_qps": args.serve,
+        "queries": len(wl.queries), "served_qps": len(wl.queries) / span,
+        "latency_ms": {"p50": float(np.percentile(ms, 50)), "p90": float(np.percentile(ms, 90)),
+                       "p99": float(np.percentile(ms, 99)), "max": float(ms.max())},
+        "results_equal_alone": got == [r.cost for r in alone]}), flush=True)
+
+
 def _port_range(wl, queries):
     import oracle
     for q in queries:
@@ -230,8 +310,15 @@ def main():
     ap.add_argument("--arena-gb", type=float, default=0.0, help="device arena size (0: 85%% of free memory)")
     ap.add_argument("--max-slots", type=int, default=0, help="queries resident at once (0: engine default)")
     ap.add_argument("--rounds-per-poll", type=int, default=0)
+    ap.add_argument("--bucket-shift", type=int, default=0, help="cost-bucket width = best >> shift (0: engine default)")
+    ap.add_argument("--ref-gpu", type=int, default=0,
+                    help="also run the reference GPU TrimCDP on this many plain queries (comparator)")
+    ap.add_argument("--serve", type=float, default=0.0,
+                    help="serving mode: Poisson arrivals at this many queries/s (prints its own line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.serve > 0:
+        return run_serving(args)
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -256,7 +343,8 @@ def main():
     queries = [q for q, _ in wl.queries]
     Ds = [D for _, D in wl.queries]
     eng = gst_b200.Engine(device=local, profile=True, arena_bytes=int(args.arena_gb * (1 << 30)),
-                          max_slots=args.max_slots, rounds_per_poll=args.rounds_per_poll)
+                          max_slots=args.max_slots, rounds_per_poll=args.rounds_per_poll,
+                          bucket_shift=args.bucket_shift)
     eng.load_graph(wl.graph.rowptr, wl.graph.col, wl.graph.w)
     eng.load_groups(wl.groups.ptr, wl.groups.mem)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -363,6 +451,15 @@ def main():
                       f"PrunedDP++ processes on disjoint query ranges (wall clock incl. graph load); "
                       f"reference-internal time per query median "
                       f"{statistics.median(times) if times else float('nan'):.3f} s"}
+    if rank == 0 and args.ref_gpu > 0:
+        eng.close()
+        torch.cuda.empty_cache()
+        ref = reference_gpu_sample(wl, args.workload, args.ref_gpu)
+        if ref is not None:
+            plain = [i for i, (q, D) in enumerate(wl.queries) if D < 0 and len(q) == ref["k"]]
+            ref["costs_equal_ours"] = ref.pop("costs") == [costs[i] for i in plain[: ref["queries"]]]
+            ref["queries_per_s_relax_loop_only"] = ref["queries"] / ref["relax_loop_s_total"]
+            out["reference_gpu_trimcdp"] = ref
     if rank == 0:
         print(json.dumps(out), flush=True)
     eng.close()

@@ -150,6 +150,7 @@ class Engine {
     max_slots_ = c.max_slots > 0 ? std::min(c.max_slots, MAXSLOTS) : MAXSLOTS;
     max_rounds_override_ = c.max_rounds > 0 ? c.max_rounds : 0;
     profile_ = c.profile != 0;
+    bucket_shift_ = c.bucket_shift > 0 ? std::min(c.bucket_shift, 30) : 3;
     rounds_per_poll_ = c.rounds_per_poll > 0 ? c.rounds_per_poll : 8;
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
@@ -159,6 +160,11 @@ class Engine {
     cudaDeviceProp prop;
     GST_CUDA(cudaGetDeviceProperties(&prop, device_));
     num_sms_ = prop.multiProcessorCount;
+    {  // the grow kernel runs one resident wave: grid = SMs x resident blocks
+      int per_sm = 0;
+      GST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grow, GROW_WARPS * 32, 0));
+      grow_grid_ = num_sms_ * std::max(per_sm, 1);
+    }
     GST_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     SubsetTables st;
     fill_subset_tables(st);
@@ -225,6 +231,18 @@ class Engine {
     if (E) GST_CUDA(cudaMemcpy(d_adj_, adj.data(), sizeof(int2) * E, cudaMemcpyHostToDevice));
     V_ = V;
     E_ = E;
+    {  // bucket width of the cost-ordered grows: the typical lightest edge
+      double sum = 0;
+      int64_t n = 0;
+      for (int64_t v = 0; v < V; ++v) {
+        if (rowptr[v + 1] == rowptr[v]) continue;
+        int mn = INT32_MAX;
+        for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j) mn = std::min(mn, w[j]);
+        sum += mn;
+        ++n;
+      }
+      delta_ = std::max(1, (int)(n ? sum / n + 0.5 : 1));
+    }
     cache_.clear();
     drop_graph_exec();  // the captured rounds hold the old graph's pointers
     return setup_arena();
@@ -379,7 +397,8 @@ class Engine {
   size_t slab_bytes(Shape sh, Slab* out) const {
     const size_t V = (size_t)V_, E = (size_t)E_;
     const size_t W = (size_t)1 << sh.k, L = (size_t)sh.L;
-    const size_t nq = sh.L == 1 ? 2 : L;
+    const size_t nq = sh.L == 1 ? 4 : L;      // plain: near 0/1, far 2/3
+    const size_t planes = sh.L == 1 ? 2 : L;  // plain: near and far dirty planes
     Slab s;
     s.shape = sh;
     s.chunk_cap = (long long)(V + E / 32 + 64);
@@ -391,7 +410,7 @@ class Engine {
       return o;
     };
     size_t o_table = take(V * W * L * 4);
-    size_t o_mask = take(L * V * 8);
+    size_t o_mask = take(planes * V * 8);
     size_t o_queue = take(nq * V * 4);
     size_t o_touched = take(V * 4);
     size_t o_tflag = take(V * 4);
@@ -477,7 +496,7 @@ class Engine {
     s.bytes = bytes;
     const size_t V = (size_t)V_, W = (size_t)1 << sh.k, L = (size_t)sh.L;
     if (cudaMemsetAsync(s.table, 0x3f, V * W * L * 4, stream_) != cudaSuccess ||
-        cudaMemsetAsync(s.mask, 0, L * V * 8, stream_) != cudaSuccess ||
+        cudaMemsetAsync(s.mask, 0, (sh.L == 1 ? 2 : L) * V * 8, stream_) != cudaSuccess ||
         cudaMemsetAsync(s.tflag, 0, V * 4, stream_) != cudaSuccess) {
       arena_alloc_.release(off, bytes);
       return false;
@@ -529,10 +548,15 @@ class Engine {
       q.action = A_INIT;
       q.s = 1;
       q.d = 0;
-      q.cur = 1;
+      q.cur = 0;
       q.best = INF;
       q.R1 = INF / 2;
       q.answer = ~0ull;
+      q.delta = delta_;  // plain: first bucket opens at the seeds (cost 0)
+      q.bshift = bucket_shift_;
+      q.T = 0;
+      q.next_min = INF;
+      q.fcur = 2;
       GST_CUDA(cudaMemcpyAsync(d_slots_ + t, &q, sizeof(Slot), cudaMemcpyHostToDevice, stream_));
       prof_.h2d_bytes += sizeof(Slot);
       GST_CUDA(cudaStreamSynchronize(stream_));  // h_slot_ is reused
@@ -575,7 +599,7 @@ class Engine {
     k_prep<<<grid, 256, 0, st>>>(d_slots_, d_plan_, g);
     k_ctl_b<<<1, MAXSLOTS, 0, st>>>(d_slots_, d_plan_);
     if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 2], st, cudaEventRecordExternal);
-    k_grow<<<grid, GROW_WARPS * 32, 0, st>>>(d_slots_, d_plan_, g);
+    k_grow<<<grow_grid_, GROW_WARPS * 32, 0, st>>>(d_slots_, d_plan_, g);
     if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 3], st, cudaEventRecordExternal);
   }
 
@@ -715,6 +739,7 @@ class Engine {
 
   int device_ = -1;
   int num_sms_ = 0;
+  int grow_grid_ = 0;
   int max_slots_ = 256;
   int rounds_per_poll_ = 8;
   cudaStream_t stream_ = nullptr;
@@ -730,6 +755,8 @@ class Engine {
   long long* d_gptr_ = nullptr;
   int32_t* d_gmem_ = nullptr;
   int64_t V_ = 0, E_ = 0, G_ = 0;
+  int delta_ = 1;
+  int bucket_shift_ = 3;
   std::vector<int64_t> gsize_;
   std::vector<int32_t> gfirst_;
   char* arena_ = nullptr;

@@ -11,8 +11,10 @@
 //                          the labels of one (v, S) share a sector.
 //   mask[l][v]            uint64 dirty bits over the ranks of the current
 //                          layer's sets: (v, S, l) improved and must be grown.
-//   queue[qi][v]          frontier vertex lists (plain: 2 ping-pong lists;
-//                          D-: one list per depth label).
+//                          Plain problem: plane 0 holds "near" bits (cost below
+//                          the bucket bound T), plane 1 "far" bits.
+//   queue[qi][v]          frontier vertex lists (plain: near lists 0/1 and far
+//                          lists 2/3, ping-pong; D-: one list per depth label).
 //   touched[], tflag[v]   vertices that ever held a finite entry.
 //   chunks[]              the current round's grow work: (v, edge range, mask).
 //
@@ -84,6 +86,11 @@ struct Slot {
   int32_t err;
   int32_t ntouched, nchunks, nwedges;
   int32_t rounds;
+  // cost-ordered grows (plain problem): states below the bucket bound T are
+  // expanded from the near lists; costlier ones wait in the far list fcur
+  // (next_min = their smallest cost) until the near lists run dry; farround
+  // marks a round that drains the previous far list
+  int32_t delta, bshift, T, next_min, fcur, farround;
   int32_t qcount[MAXQ];
   unsigned long long answer;  // (cost << 32) | root
   unsigned long long st_frontier, st_relax, st_improve, st_merges;

@@ -64,6 +64,22 @@ __device__ __forceinline__ void mark_dirty(Slot& q, long long V, uint32_t u, int
   }
 }
 
+// Plain problem: marks (u, rank r) with cost c dirty in the near plane if c is
+// below the bucket bound T, else in the far plane (and far list).
+__device__ __forceinline__ void mark_plain(Slot& q, long long V, uint32_t u, int r, int c) {
+  if (c < q.T) {
+    mark_dirty(q, V, u, r, 0, q.cur ^ 1);
+  } else {
+    const unsigned long long om = atomicOr(&q.mask[V + u], 1ull << r);
+    if (om == 0ull) {
+      const int pos = atomicAdd(&q.qcount[q.fcur], 1);
+      if (pos < V) q.queue[(long long)q.fcur * V + pos] = u;
+      else q.err = ERR_QUEUE_CAP;
+    }
+    atomicMin(&q.next_min, c);
+  }
+}
+
 // Distance lower bound of v to singleton group i: entries above R1 only tell
 // that the distance exceeds R1.
 __device__ __forceinline__ int clip_dist(int d, int R1) { return d > R1 ? R1 + 1 : d; }
@@ -121,7 +137,8 @@ __global__ void k_init_seeds(Slot* slots, int t, Graph g) {
     uint32_t v = (uint32_t)g.gmem[g.gptr[q.groups[i]] + rem];
     q.table[(long long)v * rowlen + (1 + i) * L + 0] = 0;
     touch(q, v);
-    mark_dirty(q, g.V, v, i, 0, 0);
+    if (q.D >= 0) mark_dirty(q, g.V, v, i, 0, 0);
+    else mark_plain(q, g.V, v, i, 0);
   }
   (void)L;
 }
@@ -165,16 +182,22 @@ __global__ void k_ctl_a(Slot* slots, int nslots, Plan* plan, SlotStatus* status)
       } else {
         bool done = false;
         switch (pa) {
-          case A_INIT: if (!hop) q.cur ^= 1; else q.d = 0; break;
+          case A_INIT: if (hop) q.d = 0; break;
           case A_GROW:
-            if (!hop) { q.qcount[q.cur] = 0; q.cur ^= 1; }
-            else { q.qcount[q.d] = 0; q.d += 1; }
+            if (!hop) {
+              q.qcount[q.farround ? (q.fcur ^ 1) : q.cur] = 0;  // the list this round consumed
+              q.cur ^= 1;
+            } else {
+              q.qcount[q.d] = 0;
+              q.d += 1;
+            }
             break;
-          case A_MERGE: if (!hop) q.cur ^= 1; else q.d = 0; break;
+          case A_MERGE: if (hop) q.d = 0; break;
           case A_MERGEFULL: q.phase = PH_DONE; done = true; break;
           default: break;
         }
         q.nchunks = 0;
+        q.farround = 0;
         if (!done) {
           if (pa == A_LBPREP) {
             q.s = 2;
@@ -183,6 +206,16 @@ __global__ void k_ctl_a(Slot* slots, int nslots, Plan* plan, SlotStatus* status)
             bool more;
             if (!hop) {
               more = q.qcount[q.cur] > 0;
+              if (!more && q.qcount[q.fcur] > 0) {
+                // the bucket is drained: open the next one at the cheapest
+                // waiting state and drain the far list into it
+                const int width = q.best < INF ? imax(q.delta, q.best >> q.bshift) : q.delta;
+                q.T = q.next_min + width;
+                q.next_min = INF;
+                q.fcur ^= 1;
+                q.farround = 1;
+                more = true;
+              }
             } else {
               while (q.d < q.D && q.qcount[q.d] == 0) q.d++;
               more = q.d < q.D;
@@ -198,7 +231,7 @@ __global__ void k_ctl_a(Slot* slots, int nslots, Plan* plan, SlotStatus* status)
           }
           if (act == A_MERGE || act == A_MERGEFULL)  // one item per (touched vertex, set of the layer)
             n_merge = (long long)q.ntouched * (c_sub.loff[q.k][q.s + 1] - c_sub.loff[q.k][q.s]);
-          if (act == A_GROW) n_prep = hop ? q.qcount[q.d] : q.qcount[q.cur];
+          if (act == A_GROW) n_prep = hop ? q.qcount[q.d] : q.qcount[q.farround ? (q.fcur ^ 1) : q.cur];
         }
       }
       q.action = act;
@@ -429,12 +462,29 @@ __device__ __forceinline__ void merge_costs(const int32_t* row, int k, int S, in
 
 template <int LT>
 __device__ __forceinline__ void merge_item(Slot& q, int t, uint32_t v, int r, Graph& g,
-                                           unsigned long long* ans, unsigned long long* dirty0) {
+                                           unsigned long long* ans, unsigned long long* dirty0, int* dmin) {
   const int k = q.k, W = q.W, L = LT > 0 ? LT : q.L, rowlen = W * L, D = q.D, s = q.s;
   const bool hop = D >= 0;
   const int lo = c_sub.loff[k][s];
   const int S = c_sub.sof[k][lo + r];
   int32_t* row = q.table + (long long)v * rowlen;
+  const int best = *(volatile int*)&q.best;
+  int dist[MAXK];
+  int lbv = 0;
+  if (s < k) {
+    // a tree rooted at v that covers S reaches every group of S, so its cost
+    // is at least max_{i in S} dist_i(v): skip the split loop when even that
+    // cannot pass the lower-bound test
+    int need = 0;
+    for (int i = 0; i < k; ++i) {
+      int dm = INF;
+      for (int l = 0; l < L; ++l) dm = imin(dm, row[(1 + i) * L + l]);
+      dist[i] = clip_dist(dm, q.R1);
+      if ((S >> i) & 1) need = imax(need, dist[i]);
+    }
+    lbv = lower_bound(dist, k, W, S, q.lbtab);
+    if ((long long)need + lbv > best) return;
+  }
   int M[LT > 0 ? LT : MAXL];
   merge_costs<LT>(row, k, S, L, D, M);
   if (s == k) {
@@ -442,14 +492,6 @@ __device__ __forceinline__ void merge_item(Slot& q, int t, uint32_t v, int r, Gr
     if (a < INF) *ans = ((unsigned long long)(unsigned)a << 32) | (unsigned long long)v;
     return;
   }
-  const int best = *(volatile int*)&q.best;
-  int dist[MAXK];
-  for (int i = 0; i < k; ++i) {
-    int dm = INF;
-    for (int l = 0; l < L; ++l) dm = imin(dm, row[(1 + i) * L + l]);
-    dist[i] = clip_dist(dm, q.R1);
-  }
-  const int lbv = lower_bound(dist, k, W, S, q.lbtab);
   for (int l = 0; l < L; ++l) {
     const int val = M[l];
     if (val >= INF) continue;
@@ -468,8 +510,12 @@ __device__ __forceinline__ void merge_item(Slot& q, int t, uint32_t v, int r, Gr
       }
     if (ub < best) atomicMin(&q.best, (int)ub);
     if (2LL * val <= best && (!hop || l < D)) {
-      if (!hop) *dirty0 |= 1ull << r;  // plain: aggregated per vertex by the caller
-      else mark_dirty(q, g.V, v, r, l, l);
+      if (!hop) {  // plain: aggregated per vertex by the caller
+        *dirty0 |= 1ull << r;
+        *dmin = imin(*dmin, val);
+      } else {
+        mark_dirty(q, g.V, v, r, l, l);
+      }
     }
   }
   (void)t;
@@ -490,6 +536,7 @@ k_merge(Slot* slots, const Plan* plan, Graph g) {
   const long long span = (total + 31) & ~31ll;
   for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < span; gi += stride) {
     unsigned long long ans = ~0ull, dirty = 0, key = ~0ull;
+    int dmin = INF;
     int t = -1;
     uint32_t v = 0;
     unsigned long long nsplit = 0;
@@ -504,12 +551,12 @@ k_merge(Slot* slots, const Plan* plan, Graph g) {
       v = q.touched[vi];
       key = ((unsigned long long)(unsigned)t << 32) | (unsigned)vi;
       switch (q.L) {
-        case 1: merge_item<1>(q, t, v, r, g, &ans, &dirty); break;
-        case 3: merge_item<3>(q, t, v, r, g, &ans, &dirty); break;
-        case 4: merge_item<4>(q, t, v, r, g, &ans, &dirty); break;
-        case 5: merge_item<5>(q, t, v, r, g, &ans, &dirty); break;
-        case 6: merge_item<6>(q, t, v, r, g, &ans, &dirty); break;
-        default: merge_item<0>(q, t, v, r, g, &ans, &dirty); break;
+        case 1: merge_item<1>(q, t, v, r, g, &ans, &dirty, &dmin); break;
+        case 3: merge_item<3>(q, t, v, r, g, &ans, &dirty, &dmin); break;
+        case 4: merge_item<4>(q, t, v, r, g, &ans, &dirty, &dmin); break;
+        case 5: merge_item<5>(q, t, v, r, g, &ans, &dirty, &dmin); break;
+        case 6: merge_item<6>(q, t, v, r, g, &ans, &dirty, &dmin); break;
+        default: merge_item<0>(q, t, v, r, g, &ans, &dirty, &dmin); break;
       }
       const int S = c_sub.sof[k][lo + r];
       nsplit = (1ull << (__popc(S) - 1)) - 1;
@@ -521,17 +568,20 @@ k_merge(Slot* slots, const Plan* plan, Graph g) {
     const bool shead = seg_head(skey);
     const bool vhead = seg_head(key);
     if (t >= 0 && shead && amin != ~0ull) atomicMin(&slots[t].answer, amin);
-    // plain dirty bits: one atomicOr (and at most one enqueue) per (warp, vertex)
+    // plain seeds: one atomicOr (and at most one enqueue) per (warp, vertex),
+    // into the far plane; the next grow round opens the first bucket at the
+    // cheapest seed
     const unsigned long long dor = seg_or_u64(dirty, key);
+    const unsigned long long dm = seg_min_u64((unsigned long long)(unsigned)dmin, key);
     if (t >= 0 && vhead && dor) {
       Slot& q = slots[t];
-      const unsigned long long om = atomicOr(&q.mask[v], dor);
+      const unsigned long long om = atomicOr(&q.mask[g.V + v], dor);
       if (om == 0ull) {
-        const int qi = q.cur ^ 1;
-        const int pos = atomicAdd(&q.qcount[qi], 1);
-        if (pos < g.V) q.queue[(long long)qi * g.V + pos] = v;
+        const int pos = atomicAdd(&q.qcount[q.fcur], 1);
+        if (pos < g.V) q.queue[(long long)q.fcur * g.V + pos] = v;
         else q.err = ERR_QUEUE_CAP;
       }
+      atomicMin(&q.next_min, (int)dm);
     }
     const unsigned long long ns = seg_add_u64(nsplit, skey);
     if (t >= 0 && shead && ns) atomicAdd(&slots[t].st_merges, ns);
@@ -551,19 +601,43 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
     const int j = seg_search(plan->prep_off, ng, gi);
     Slot& q = slots[plan->grow_slots[j]];
     const bool hop = q.D >= 0;
+    const bool farround = !hop && q.farround;
     const int lvl = hop ? q.d : 0;
-    const int qi = hop ? q.d : q.cur;
+    const int qi = hop ? q.d : (farround ? (q.fcur ^ 1) : q.cur);
     const uint32_t v = q.queue[(long long)qi * g.V + (gi - plan->prep_off[j])];
-    unsigned long long m = atomicExch(&q.mask[(long long)lvl * g.V + v], 0ull);
+    const long long plane = hop ? lvl : (farround ? 1 : 0);
+    unsigned long long m = atomicExch(&q.mask[plane * g.V + v], 0ull);
     if (m == 0ull) continue;
-    {  // keep the sets whose cost is still a valid grow source (2 * cost <= best)
+    {
+      // keep the sets whose cost is still a valid grow source (2 * cost <= best);
+      // plain problem: expand only costs below the bucket bound T and put the
+      // others back on the far list (cost order: a state is expanded once it
+      // is final rather than every time it improves)
       const int best = *(volatile int*)&q.best;
       const int k = q.k, L = q.L, lo = c_sub.loff[k][q.s];
+      const int T = hop ? INF : q.T;
       const int32_t* src = q.table + (long long)v * q.W * L;
+      unsigned long long far = 0;
+      int fmin = INF;
       for (unsigned long long x = m; x; x &= x - 1) {
         const int r = __ffsll((long long)x) - 1;
         const int sv = src[(lo + r) * L + lvl];
-        if (sv >= INF || 2LL * sv > best) m &= ~(1ull << r);
+        if (sv >= INF || 2LL * sv > best) {
+          m &= ~(1ull << r);
+        } else if (sv >= T) {
+          m &= ~(1ull << r);
+          far |= 1ull << r;
+          fmin = imin(fmin, sv);
+        }
+      }
+      if (far) {
+        const unsigned long long om = atomicOr(&q.mask[g.V + v], far);
+        if (om == 0ull) {
+          const int pos = atomicAdd(&q.qcount[q.fcur], 1);
+          if (pos < g.V) q.queue[(long long)q.fcur * g.V + pos] = v;
+          else q.err = ERR_QUEUE_CAP;
+        }
+        atomicMin(&q.next_min, fmin);
       }
     }
     if (m == 0ull) continue;
@@ -732,8 +806,10 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
           ++nimp;
           touch(q, u);
           if (s == 1 && (!hop || td <= D / 2)) star_bound(q, trow, k, L, hop ? D / 2 : 0);
-          if (2LL * nc[i] <= best && (!hop || td < D))
-            mark_dirty(q, g.V, u, r, hop ? td : 0, hop ? td : (q.cur ^ 1));
+          if (2LL * nc[i] <= best) {
+            if (!hop) mark_plain(q, g.V, u, r, nc[i]);
+            else if (td < D) mark_dirty(q, g.V, u, r, td, td);
+          }
         }
       }
     }
@@ -918,11 +994,12 @@ __global__ void k_reset(Slot* slots, int t, Graph g) {
     const uint32_t v = q.touched[x / rowlen];
     q.table[(long long)v * rowlen + (x % rowlen)] = INF;
   }
-  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < (long long)n * L;
+  const int planes = q.D >= 0 ? L : 2;  // plain: near and far planes
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < (long long)n * planes;
        x += (long long)gridDim.x * blockDim.x) {
-    const uint32_t v = q.touched[x / L];
-    q.mask[(x % L) * g.V + v] = 0ull;
-    if (x % L == 0) q.tflag[v] = 0u;
+    const uint32_t v = q.touched[x / planes];
+    q.mask[(x % planes) * g.V + v] = 0ull;
+    if (x % planes == 0) q.tflag[v] = 0u;
   }
 }
 

@@ -145,7 +145,8 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   }
 
   // carve the scratch array
-  const size_t W = (size_t)1 << kk, L = D < 0 ? 1 : (size_t)D + 1, nq = D < 0 ? 2 : L;
+  const size_t W = (size_t)1 << kk, L = D < 0 ? 1 : (size_t)D + 1, nq = D < 0 ? 4 : L;
+  const size_t planes = D < 0 ? 2 : L;  // plain: near and far dirty planes
   const size_t chunk_cap = (size_t)V + (size_t)E / 32 + 64;
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off += up256(bytes); return o; };
@@ -153,7 +154,7 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   const size_t o_plan = take(sizeof(Plan));
   const size_t o_status = take(sizeof(SlotStatus));
   const size_t o_table = take((size_t)V * W * L * 4);
-  const size_t o_mask = take(L * (size_t)V * 8);
+  const size_t o_mask = take(planes * (size_t)V * 8);
   const size_t o_queue = take(nq * (size_t)V * 4);
   const size_t o_touched = take((size_t)V * 4);
   const size_t o_tflag = take((size_t)V * 4);
@@ -187,14 +188,19 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   q.phase = PH_ACTIVE;
   q.action = A_INIT;
   q.s = 1;
-  q.cur = 1;
+  q.cur = 0;
   q.best = INF;
   q.R1 = INF / 2;
   q.answer = ~0ull;
+  q.delta = 1;  // narrow first buckets: correct for any weights without a pass over the graph
+  q.bshift = 3;
+  q.T = 0;
+  q.next_min = INF;
+  q.fcur = 2;
 
   // what must start cleared: the table (INF), dirty masks, touched flags, plan
   ce = cudaMemsetAsync(base + o_table, 0x3f, (size_t)V * W * L * 4, s);
-  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_mask, 0, L * (size_t)V * 8, s);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_mask, 0, planes * (size_t)V * 8, s);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_tflag, 0, (size_t)V * 4, s);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(d_plan, 0, sizeof(Plan), s);
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_slot, &q, sizeof q, cudaMemcpyHostToDevice, s);

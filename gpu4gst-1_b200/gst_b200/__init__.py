@@ -63,7 +63,7 @@ class _Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("arena_fraction", ctypes.c_double),
                 ("arena_bytes", ctypes.c_int64), ("max_slots", ctypes.c_int),
                 ("rounds_per_poll", ctypes.c_int), ("max_rounds", ctypes.c_int),
-                ("profile", ctypes.c_int)]
+                ("profile", ctypes.c_int), ("bucket_shift", ctypes.c_int)]
 
 
 class _Profile(ctypes.Structure):
@@ -233,10 +233,10 @@ class Engine:
 
     def __init__(self, device: int = 0, arena_fraction: float = 0.0, arena_bytes: int = 0,
                  max_slots: int = 0, rounds_per_poll: int = 0, max_rounds: int = 0,
-                 profile: bool = False):
+                 profile: bool = False, bucket_shift: int = 0):
         self._lib = load_library()
         cfg = _Config(device, arena_fraction, arena_bytes, max_slots, rounds_per_poll, max_rounds,
-                      1 if profile else 0)
+                      1 if profile else 0, bucket_shift)
         h = ctypes.c_void_p()
         _check(self._lib.gst_engine_create(ctypes.byref(cfg), ctypes.byref(h)), "engine_create")
         self._h = h

@@ -1,0 +1,87 @@
+"""Parity at the benchmark sizes (C2: 170k vertices, k=5; a C3-shaped
+diameter-bounded k=7 case) through size-independent properties, plus a sample
+against the oracle restatement where it finishes in seconds.
+
+* every returned tree is a tree of exactly the reported weight touching every
+  group (and of hop diameter <= D for the D- variants);
+* the batch and the one-query-per-call forms agree;
+* permuting a query's group ids does not change the cost;
+* costs are non-increasing in D and never below the plain optimum;
+* on C2, a sample of queries equals the PrunedDP++ restatement."""
+import numpy as np
+import pytest
+
+import gst_b200
+from gst_b200 import datagen as dg
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c2():
+    wl = dg.config_c2(1, n_queries=24)
+    e = gst_b200.Engine(device=0, arena_bytes=8 << 30, max_rounds=500000)
+    e.load_graph(wl.graph.rowptr, wl.graph.col, wl.graph.w)
+    e.load_groups(wl.groups.ptr, wl.groups.mem)
+    yield wl, e
+    e.close()
+
+
+def test_c2_trees_batch_single_permutation(c2):
+    wl, e = c2
+    qs = [q for q, _ in wl.queries]
+    batch = e.solve_batch(qs)
+    rng = np.random.default_rng(11)
+    for i, (q, r) in enumerate(zip(qs, batch)):
+        assert r.status == 0 and r.feasible
+        assert oracle.validate(wl.graph, wl.groups, q, r.edges, r.root, r.cost) == 0
+        if i < 6:
+            assert e.solve(q).cost == r.cost
+            assert e.solve(rng.permutation(q)).cost == r.cost
+
+
+def test_c2_sample_equals_prunedpp_restatement(c2):
+    wl, e = c2
+    for q, _ in wl.queries[:2]:
+        want = oracle.prunedpp(wl.graph, wl.groups, q)[0]
+        assert e.solve(q).cost == want
+
+
+def test_c2_diameter_bound_properties(c2):
+    wl, e = c2
+    for q, _ in wl.queries[:4]:
+        plain = e.solve(q).cost
+        prev = None
+        for D in (2, 3, 4, 5, 8):
+            r = e.solve(q, D)
+            if r.feasible:
+                assert oracle.validate(wl.graph, wl.groups, q, r.edges, r.root, r.cost, D) == 0
+                assert r.cost >= plain
+            if prev is not None:
+                assert r.cost <= prev
+            prev = r.cost
+
+
+def test_c3_shaped_k7_diameter_bound():
+    """1M-vertex BA graph (m=10, w U[1,1000]), k=7, D in {2..5}: trees valid,
+    costs non-increasing in D, batch equals single."""
+    g = dg.ba_graph(1_000_000, 10, 1, 1000, seed=1)
+    gr = dg.make_groups(g.V, 10_000, seed=101, geometric=(10, 2, 500))
+    qs = [q for q, _ in dg.make_queries(gr.n, 3, 7, seed=201)]
+    e = gst_b200.Engine(device=0, arena_bytes=48 << 30, max_rounds=500000)
+    e.load_graph(g.rowptr, g.col, g.w)
+    e.load_groups(gr.ptr, gr.mem)
+    for q in qs:
+        costs = []
+        for D in (2, 3, 4, 5):
+            r = e.solve(q, D)
+            assert r.status == 0
+            if r.feasible:
+                assert oracle.validate(g, gr, q, r.edges, r.root, r.cost, D) == 0
+            costs.append(r.cost)
+        assert all(a >= b for a, b in zip(costs, costs[1:]))
+    batch = e.solve_batch(qs, [3, 4, 5])
+    for q, D, r in zip(qs, [3, 4, 5], batch):
+        assert r.cost == e.solve(q, D).cost
+    e.close()
