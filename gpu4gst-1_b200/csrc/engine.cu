@@ -150,7 +150,7 @@ class Engine {
     max_slots_ = c.max_slots > 0 ? std::min(c.max_slots, MAXSLOTS) : MAXSLOTS;
     max_rounds_override_ = c.max_rounds > 0 ? c.max_rounds : 0;
     profile_ = c.profile != 0;
-    bucket_shift_ = c.bucket_shift > 0 ? std::min(c.bucket_shift, 30) : 3;
+    bucket_shift_ = c.bucket_shift > 0 ? std::min(c.bucket_shift, 30) : 30;
     rounds_per_poll_ = c.rounds_per_poll > 0 ? c.rounds_per_poll : 8;
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
@@ -756,7 +756,7 @@ class Engine {
   int32_t* d_gmem_ = nullptr;
   int64_t V_ = 0, E_ = 0, G_ = 0;
   int delta_ = 1;
-  int bucket_shift_ = 3;
+  int bucket_shift_ = 30;
   std::vector<int64_t> gsize_;
   std::vector<int32_t> gfirst_;
   char* arena_ = nullptr;

@@ -193,7 +193,7 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   q.R1 = INF / 2;
   q.answer = ~0ull;
   q.delta = 1;  // narrow first buckets: correct for any weights without a pass over the graph
-  q.bshift = 3;
+  q.bshift = 30;
   q.T = 0;
   q.next_min = INF;
   q.fcur = 2;

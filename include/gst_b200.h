@@ -113,7 +113,8 @@ typedef struct {
                               GST_E_LIMIT (0: unlimited) */
   int profile;             /* 1: time the grow and merge kernels with CUDA events */
   int bucket_shift;        /* plain grows run in cost buckets of width
-                              max(lightest edge, best >> bucket_shift) (0 -> 3) */
+                              max(typical lightest edge, best >> bucket_shift)
+                              (0 -> 30: the lightest-edge width, best measured) */
 } gst_engine_config;
 
 gst_status gst_engine_create(const gst_engine_config* cfg, gst_engine** out);
