@@ -63,6 +63,20 @@ def make_workload(name: str, rank: int):
     return wl
 
 
+def filter_queries(wl, args):
+    """Optional sub-selection of a workload's queries (profiling small cases)."""
+    qs = wl.queries
+    if args.k > 0:
+        qs = [(q, D) for q, D in qs if len(q) == args.k]
+    if args.kind == "plain":
+        qs = [(q, D) for q, D in qs if D < 0]
+    elif args.kind == "hop":
+        qs = [(q, D) for q, D in qs if D >= 0]
+    if args.queries > 0:
+        qs = qs[: args.queries]
+    wl.queries = qs
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -224,8 +238,7 @@ def run_serving(args):
     import numpy as np
     import gst_b200
     wl = make_workload(args.workload, 0)
-    if args.queries > 0:
-        wl.queries = wl.queries[: args.queries]
+    filter_queries(wl, args)
     eng = gst_b200.Engine(device=0, arena_bytes=int(args.arena_gb * (1 << 30)))
     eng.load_graph(wl.graph.rowptr, wl.graph.col, wl.graph.w)
     eng.load_groups(wl.groups.ptr, wl.groups.mem)
@@ -311,6 +324,9 @@ def main():
     ap.add_argument("--max-slots", type=int, default=0, help="queries resident at once (0: engine default)")
     ap.add_argument("--rounds-per-poll", type=int, default=0)
     ap.add_argument("--bucket-shift", type=int, default=0, help="cost-bucket width = best >> shift (0: engine default)")
+    ap.add_argument("--k", type=int, default=0, help="keep only queries with this many groups (0: all)")
+    ap.add_argument("--kind", default="all", choices=["all", "plain", "hop"],
+                    help="keep only plain (D unbounded) or diameter-bounded queries")
     ap.add_argument("--ref-gpu", type=int, default=0,
                     help="also run the reference GPU TrimCDP on this many plain queries (comparator)")
     ap.add_argument("--serve", type=float, default=0.0,
@@ -338,8 +354,7 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     wl = make_workload(args.workload, rank)
-    if args.queries > 0:
-        wl.queries = wl.queries[: args.queries]
+    filter_queries(wl, args)
     queries = [q for q, _ in wl.queries]
     Ds = [D for _, D in wl.queries]
     eng = gst_b200.Engine(device=local, profile=True, arena_bytes=int(args.arena_gb * (1 << 30)),
@@ -423,6 +438,8 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded BA power-law graphs standing in for the reference's external datasets)",
         "config": {"workload": WORKLOADS[args.workload], "queries_per_step_per_gpu": nq,
+                   **({"query_filter": f"k={args.k or 'any'} kind={args.kind} first={args.queries or 'all'}"}
+                      if (args.k or args.kind != "all" or args.queries) else {}),
                    "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before every step; "
                    "per-query DP tables (hundreds of MB per step) exceed L2"},
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,

@@ -800,11 +800,16 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
           const int r = rr[i];
           int32_t* trow = q.table + (long long)u * rowlen;
           const long long tidx = (long long)(lo + r) * L;
-          if (s >= 2 && lb_prunes(trow, k, W, L, c_sub.sof[k][lo + r], q.R1, q.lbtab, nc[i], best)) continue;
+          // A candidate that fails the lower-bound test is still a real
+          // derivation cost: store it (unmarked, so never grown from) so that
+          // later, costlier candidates for this state stop at the read above
+          // instead of re-running the bound.
+          const bool pruned = s >= 2 && lb_prunes(trow, k, W, L, c_sub.sof[k][lo + r], q.R1, q.lbtab, nc[i], best);
           const int old = atomicMin(&trow[tidx + td], nc[i]);
           if (old <= nc[i]) continue;
-          ++nimp;
           touch(q, u);
+          if (pruned) continue;
+          ++nimp;
           if (s == 1 && (!hop || td <= D / 2)) star_bound(q, trow, k, L, hop ? D / 2 : 0);
           if (2LL * nc[i] <= best) {
             if (!hop) mark_plain(q, g.V, u, r, nc[i]);
