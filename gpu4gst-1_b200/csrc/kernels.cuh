@@ -56,7 +56,10 @@ __device__ __forceinline__ void touch(Slot& q, uint32_t u) {
 
 // Marks (u, rank r, label l) dirty and enqueues u on the list qi if it was clean.
 __device__ __forceinline__ void mark_dirty(Slot& q, long long V, uint32_t u, int r, int mi, int qi) {
-  unsigned long long om = atomicOr(&q.mask[(long long)mi * V + u], 1ull << r);
+  unsigned long long* mp = &q.mask[(long long)mi * V + u];
+  // within a grow or merge pass bits are only set, so a bit seen set stays set
+  if ((*(volatile unsigned long long*)mp >> r) & 1ull) return;
+  unsigned long long om = atomicOr(mp, 1ull << r);
   if (om == 0ull) {
     int pos = atomicAdd(&q.qcount[qi], 1);
     if (pos < V) q.queue[(long long)qi * V + pos] = u;
@@ -70,13 +73,18 @@ __device__ __forceinline__ void mark_plain(Slot& q, long long V, uint32_t u, int
   if (c < q.T) {
     mark_dirty(q, V, u, r, 0, q.cur ^ 1);
   } else {
-    const unsigned long long om = atomicOr(&q.mask[V + u], 1ull << r);
-    if (om == 0ull) {
-      const int pos = atomicAdd(&q.qcount[q.fcur], 1);
-      if (pos < V) q.queue[(long long)q.fcur * V + pos] = u;
-      else q.err = ERR_QUEUE_CAP;
+    unsigned long long* mp = &q.mask[V + u];
+    if (!((*(volatile unsigned long long*)mp >> r) & 1ull)) {
+      const unsigned long long om = atomicOr(mp, 1ull << r);
+      if (om == 0ull) {
+        const int pos = atomicAdd(&q.qcount[q.fcur], 1);
+        if (pos < V) q.queue[(long long)q.fcur * V + pos] = u;
+        else q.err = ERR_QUEUE_CAP;
+      }
     }
-    atomicMin(&q.next_min, c);
+    // next_min only decreases during the pass: skip the contended atomic
+    // unless this cost can lower it
+    if (c < *(volatile int*)&q.next_min) atomicMin(&q.next_min, c);
   }
 }
 
@@ -581,7 +589,7 @@ k_merge(Slot* slots, const Plan* plan, Graph g) {
         if (pos < g.V) q.queue[(long long)q.fcur * g.V + pos] = v;
         else q.err = ERR_QUEUE_CAP;
       }
-      atomicMin(&q.next_min, (int)dm);
+      if ((int)dm < *(volatile int*)&q.next_min) atomicMin(&q.next_min, (int)dm);
     }
     const unsigned long long ns = seg_add_u64(nsplit, skey);
     if (t >= 0 && shead && ns) atomicAdd(&slots[t].st_merges, ns);
@@ -637,7 +645,7 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
           if (pos < g.V) q.queue[(long long)q.fcur * g.V + pos] = v;
           else q.err = ERR_QUEUE_CAP;
         }
-        atomicMin(&q.next_min, fmin);
+        if (fmin < *(volatile int*)&q.next_min) atomicMin(&q.next_min, fmin);
       }
     }
     if (m == 0ull) continue;
@@ -697,14 +705,31 @@ __device__ __forceinline__ void flush_counts(Slot& q, unsigned long long& nrel, 
   nimp = 0;
 }
 
-// Star upper bound at a vertex that just improved a singleton entry.
-__device__ __noinline__ void star_bound(Slot& q, const int32_t* trow, int k, int L, int hl) {
-  long long ub = 0;
-  for (int i = 0; i < k && ub < INF; ++i) {
-    int dm = INF;
-    for (int l = 0; l <= hl; ++l) dm = imin(dm, trow[(1 + i) * L + l]);
-    ub += dm;
+// Star upper bound at a vertex that just improved a singleton entry: the
+// cheapest path to every group, joined at the vertex.  With a diameter bound D
+// every branch may be hl = floor(D/2) hops deep and one of them hh = ceil(D/2)
+// (any two branches then span at most D hops).
+__device__ __noinline__ void star_bound(Slot& q, const int32_t* trow, int k, int L, int hl, int hh) {
+  long long sum = 0, gain = 0;
+  int ninf = 0;
+  long long deep_only = INF;  // the one group reachable only within hh hops
+  for (int i = 0; i < k; ++i) {
+    int a = INF, b = INF;
+    for (int l = 0; l <= hh; ++l) {
+      const int x = trow[(1 + i) * L + l];
+      if (l <= hl) a = imin(a, x);
+      b = imin(b, x);
+    }
+    if (b >= INF) return;
+    if (a >= INF) {
+      if (++ninf > 1) return;
+      deep_only = b;
+    } else {
+      sum += a;
+      gain = gain < (long long)b - a ? gain : (long long)b - a;
+    }
   }
+  const long long ub = ninf ? sum + deep_only : sum + gain;
   if (ub < *(volatile int*)&q.best) atomicMin(&q.best, (int)ub);
 }
 
@@ -810,7 +835,7 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
           touch(q, u);
           if (pruned) continue;
           ++nimp;
-          if (s == 1 && (!hop || td <= D / 2)) star_bound(q, trow, k, L, hop ? D / 2 : 0);
+          if (s == 1 && (!hop || td <= (D + 1) / 2)) star_bound(q, trow, k, L, hop ? D / 2 : 0, hop ? (D + 1) / 2 : 0);
           if (2LL * nc[i] <= best) {
             if (!hop) mark_plain(q, g.V, u, r, nc[i]);
             else if (td < D) mark_dirty(q, g.V, u, r, td, td);
