@@ -94,31 +94,34 @@ __device__ __forceinline__ int clip_dist(int d, int R1) { return d > R1 ? R1 + 1
 
 // Tour / one-label lower bound for completing (v, S) given the clipped
 // singleton distances dist[0..k) of v (LB_procedure, CPUNONHOP.h:436-496).
+// The loops walk the set bits of the complement X of S, so every lane of a
+// layer (same |S|) runs the same (k - |S|)^2 iterations.  ceil(t / 2) is
+// monotone in t, so the tour bound rounds its minimum once.
 __device__ __forceinline__ int lower_bound(const int* dist, int k, int W, int S,
                                            const int32_t* lbtab) {
-  const int full = W - 1;
-  const int Xs = full ^ S;
+  const int Xs = (W - 1) ^ S;
   if (Xs == 0) return 0;
   int one = 0, mind = INF;
-  for (int i = 0; i < k; ++i)
-    if (Xs >> i & 1) {
-      one = imax(one, dist[i]);
-      mind = imin(mind, dist[i]);
+  for (int x = Xs; x; x &= x - 1) {
+    const int d = dist[__ffs(x) - 1];
+    one = imax(one, d);
+    mind = imin(mind, d);
+  }
+  long long t1 = 2LL * INF, lb2 = 0;
+  const int32_t* W2 = lbtab + (size_t)k * k * W + Xs;
+  for (int x = Xs; x; x &= x - 1) {
+    const int i = __ffs(x) - 1;
+    const long long di = dist[i];
+    const int32_t* Pi = lbtab + (size_t)i * k * W + Xs;
+    for (int y = Xs; y; y &= y - 1) {
+      const int j = __ffs(y) - 1;
+      const long long t = di + Pi[j * W] + dist[j];
+      if (t < t1) t1 = t;
     }
-  long long lb1 = INF, lb2 = 0;
-  const int32_t* W2 = lbtab + (size_t)k * k * W;
-  for (int i = 0; i < k; ++i) {
-    if (!(Xs >> i & 1)) continue;
-    for (int j = 0; j < k; ++j) {
-      if (!(Xs >> j & 1)) continue;
-      long long t = (long long)dist[i] + lbtab[(i * k + j) * W + Xs] + dist[j];
-      t = (t + 1) >> 1;
-      if (t < lb1) lb1 = t;
-    }
-    long long t2 = (long long)dist[i] + W2[i * W + Xs] + mind;
-    t2 = (t2 + 1) >> 1;
+    const long long t2 = (di + W2[i * W] + mind + 1) >> 1;
     if (t2 > lb2) lb2 = t2;
   }
+  const long long lb1 = (t1 + 1) >> 1;
   long long lb = one;
   if (lb1 > lb && lb1 < INF) lb = lb1;
   if (lb2 > lb) lb = lb2;
