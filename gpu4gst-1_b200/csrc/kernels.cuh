@@ -426,10 +426,16 @@ __device__ __forceinline__ bool seg_head(unsigned long long key) {
 }
 
 // Merged costs M[0..L) (prefix minima over labels) of set S at a vertex row.
+// sidx: the subset -> index map of this k (in shared memory: lanes look up
+// different subsets, which the constant cache would serialise).  With a
+// compile-time label count LT > 1 the bound is D = LT - 1, so the label
+// pairing below indexes registers.
 template <int LT>
-__device__ __forceinline__ void merge_costs(const int32_t* row, int k, int S, int Lrt, int D, int* M) {
+__device__ __forceinline__ void merge_costs(const int32_t* row, const uint8_t* sidx, int S, int Lrt, int Drt,
+                                            int* M) {
   const int L = LT > 0 ? LT : Lrt;
-  const int base = c_sub.sidx[k][S] * L;
+  const int D = LT > 0 ? LT - 1 : Drt;
+  const int base = sidx[S] * L;
   {
     int m = INF;
 #pragma unroll
@@ -442,7 +448,7 @@ __device__ __forceinline__ void merge_costs(const int32_t* row, int k, int S, in
   for (int S1 = (S - 1) & S; S1 > 0; S1 = (S1 - 1) & S) {
     const int S2 = S ^ S1;
     if (S1 < S2) continue;
-    const int i1 = c_sub.sidx[k][S1] * L, i2 = c_sub.sidx[k][S2] * L;
+    const int i1 = sidx[S1] * L, i2 = sidx[S2] * L;
     if (LT == 1) {
       M[0] = imin(M[0], row[i1] + row[i2]);
     } else {
@@ -472,12 +478,12 @@ __device__ __forceinline__ void merge_costs(const int32_t* row, int k, int S, in
 }
 
 template <int LT>
-__device__ __forceinline__ void merge_item(Slot& q, int t, uint32_t v, int r, Graph& g,
-                                           unsigned long long* ans, unsigned long long* dirty0, int* dmin) {
+__device__ __forceinline__ void merge_item(Slot& q, int t, uint32_t v, int r, int S, const uint8_t* sidx,
+                                           Graph& g, unsigned long long* ans, unsigned long long* dirty0,
+                                           int* dmin) {
   const int k = q.k, W = q.W, L = LT > 0 ? LT : q.L, rowlen = W * L, D = q.D, s = q.s;
   const bool hop = D >= 0;
   const int lo = c_sub.loff[k][s];
-  const int S = c_sub.sof[k][lo + r];
   int32_t* row = q.table + (long long)v * rowlen;
   const int best = *(volatile int*)&q.best;
   int dist[MAXK];
@@ -497,7 +503,7 @@ __device__ __forceinline__ void merge_item(Slot& q, int t, uint32_t v, int r, Gr
     if ((long long)need + lbv > best) return;
   }
   int M[LT > 0 ? LT : MAXL];
-  merge_costs<LT>(row, k, S, L, D, M);
+  merge_costs<LT>(row, sidx, S, L, D, M);
   if (s == k) {
     const int a = M[L - 1];
     if (a < INF) *ans = ((unsigned long long)(unsigned)a << 32) | (unsigned long long)v;
@@ -536,10 +542,15 @@ __global__ void __launch_bounds__(MERGE_THREADS)
 k_merge(Slot* slots, const Plan* plan, Graph g) {
   __shared__ long long s_off[MAXSLOTS + 1];
   __shared__ int s_slot[MAXSLOTS];
+  __shared__ uint8_t s_sidx[MAXK + 1][MAXW], s_sof[MAXK + 1][MAXW];
   const int nm = plan->n_merge;
   if (nm == 0) return;
   for (int x = threadIdx.x; x <= nm; x += blockDim.x) s_off[x] = plan->merge_off[x];
   for (int x = threadIdx.x; x < nm; x += blockDim.x) s_slot[x] = plan->merge_slots[x];
+  for (int x = threadIdx.x; x < (MAXK + 1) * MAXW; x += blockDim.x) {
+    (&s_sidx[0][0])[x] = (&c_sub.sidx[0][0])[x];
+    (&s_sof[0][0])[x] = (&c_sub.sof[0][0])[x];
+  }
   __syncthreads();
   const long long total = s_off[nm];
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -559,17 +570,19 @@ k_merge(Slot* slots, const Plan* plan, Graph g) {
       const int lo = c_sub.loff[k][s], nS = c_sub.loff[k][s + 1] - lo;
       const long long local = gi - s_off[j];
       const int vi = (int)(local / nS), r = (int)(local % nS);
+      const int S = s_sof[k][lo + r];
+      const uint8_t* sidx = s_sidx[k];
       v = q.touched[vi];
       key = ((unsigned long long)(unsigned)t << 32) | (unsigned)vi;
       switch (q.L) {
-        case 1: merge_item<1>(q, t, v, r, g, &ans, &dirty, &dmin); break;
-        case 3: merge_item<3>(q, t, v, r, g, &ans, &dirty, &dmin); break;
-        case 4: merge_item<4>(q, t, v, r, g, &ans, &dirty, &dmin); break;
-        case 5: merge_item<5>(q, t, v, r, g, &ans, &dirty, &dmin); break;
-        case 6: merge_item<6>(q, t, v, r, g, &ans, &dirty, &dmin); break;
-        default: merge_item<0>(q, t, v, r, g, &ans, &dirty, &dmin); break;
+        case 1: merge_item<1>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
+        case 2: merge_item<2>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
+        case 3: merge_item<3>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
+        case 4: merge_item<4>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
+        case 5: merge_item<5>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
+        case 6: merge_item<6>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
+        default: merge_item<0>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
       }
-      const int S = c_sub.sof[k][lo + r];
       nsplit = (1ull << (__popc(S) - 1)) - 1;
     }
     // answers: one atomic per (warp, slot).  The segment reductions and heads
@@ -780,7 +793,7 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
       const unsigned ok = __ballot_sync(0xffffffffu, r >= 0);
       if (r >= 0) {
         const int p = nact + __popc(ok & ((1u << lane) - 1));
-        s_r[wib][p] = r;
+        s_r[wib][p] = (int)c_sub.sof[k][lo + r] << 8 | r;  // (subset, rank)
         s_sv[wib][p] = sv;
       }
       nact += __popc(ok);
@@ -815,7 +828,7 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
           cur[i] = INF;
           if (nc[i] < INF) {
             const int32_t* trow = q.table + (long long)a[i].x * rowlen;
-            const long long tidx = (long long)(lo + rr[i]) * L;
+            const long long tidx = (long long)(lo + (rr[i] & 0xff)) * L;
             int cv = trow[tidx + td];
             for (int l = 0; l < td; ++l) cv = imin(cv, trow[tidx + l]);
             cur[i] = cv;
@@ -825,14 +838,14 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
         for (int i = 0; i < GROW_UNROLL; ++i) {
           if (nc[i] >= cur[i]) continue;  // also skips pairs past the end (nc = INF)
           const uint32_t u = (uint32_t)a[i].x;
-          const int r = rr[i];
+          const int r = rr[i] & 0xff;
           int32_t* trow = q.table + (long long)u * rowlen;
           const long long tidx = (long long)(lo + r) * L;
           // A candidate that fails the lower-bound test is still a real
           // derivation cost: store it (unmarked, so never grown from) so that
           // later, costlier candidates for this state stop at the read above
           // instead of re-running the bound.
-          const bool pruned = s >= 2 && lb_prunes(trow, k, W, L, c_sub.sof[k][lo + r], q.R1, q.lbtab, nc[i], best);
+          const bool pruned = s >= 2 && lb_prunes(trow, k, W, L, rr[i] >> 8, q.R1, q.lbtab, nc[i], best);
           const int old = atomicMin(&trow[tidx + td], nc[i]);
           if (old <= nc[i]) continue;
           touch(q, u);
