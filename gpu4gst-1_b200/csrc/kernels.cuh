@@ -34,6 +34,7 @@ namespace gst {
 
 __constant__ SubsetTables c_sub;
 
+
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
 
@@ -125,6 +126,25 @@ __device__ __forceinline__ int lower_bound(const int* dist, int k, int W, int S,
   long long lb = one;
   if (lb1 > lb && lb1 < INF) lb = lb1;
   if (lb2 > lb) lb = lb2;
+  return (int)(lb < INF ? lb : INF);
+}
+
+// Cheap lower bound of a tree that contains v and touches every group: the
+// one-label bound and the W2 tour bound of lower_bound with S empty (O(k);
+// the pairwise tour bound is left out).
+__device__ __forceinline__ int full_bound(const int* dist, int k, int W, const int32_t* lbtab) {
+  const int full = W - 1;
+  int one = 0, mind = INF;
+  for (int i = 0; i < k; ++i) {
+    one = imax(one, dist[i]);
+    mind = imin(mind, dist[i]);
+  }
+  long long lb = one;
+  const int32_t* W2 = lbtab + (size_t)k * k * W + full;
+  for (int i = 0; i < k; ++i) {
+    const long long t2 = ((long long)dist[i] + W2[i * W] + mind + 1) >> 1;
+    if (t2 > lb) lb = t2;
+  }
   return (int)(lb < INF ? lb : INF);
 }
 
@@ -389,6 +409,7 @@ __global__ void k_lbprep(Slot* slots, const Plan* plan, Graph g) {
 // (1 = plain); 0 handles any count.
 // ---------------------------------------------------------------------------
 constexpr int MERGE_THREADS = 256;
+constexpr int DIST_STRIDE = MAXK + (MAXK % 2 == 0 ? 1 : 0);  // odd, >= MAXK
 
 // Segmented (by key, keys contiguous in lane order) reductions; the first lane
 // of each segment ends with the result.
@@ -477,16 +498,17 @@ __device__ __forceinline__ void merge_costs(const int32_t* row, const uint8_t* s
   }
 }
 
+// Returns whether the split loop ran (false: the lower-bound pre-filter
+// rejected the item).
 template <int LT>
-__device__ __forceinline__ void merge_item(Slot& q, int t, uint32_t v, int r, int S, const uint8_t* sidx,
-                                           Graph& g, unsigned long long* ans, unsigned long long* dirty0,
-                                           int* dmin) {
+__device__ __forceinline__ bool merge_item(Slot& q, int t, uint32_t v, int r, int S, const uint8_t* sidx,
+                                           int* dist, Graph& g, unsigned long long* ans,
+                                           unsigned long long* dirty0, int* dmin) {
   const int k = q.k, W = q.W, L = LT > 0 ? LT : q.L, rowlen = W * L, D = q.D, s = q.s;
   const bool hop = D >= 0;
   const int lo = c_sub.loff[k][s];
   int32_t* row = q.table + (long long)v * rowlen;
   const int best = *(volatile int*)&q.best;
-  int dist[MAXK];
   int lbv = 0;
   if (s < k) {
     // a tree rooted at v that covers S reaches every group of S, so its cost
@@ -500,14 +522,22 @@ __device__ __forceinline__ void merge_item(Slot& q, int t, uint32_t v, int r, in
       if ((S >> i) & 1) need = imax(need, dist[i]);
     }
     lbv = lower_bound(dist, k, W, S, q.lbtab);
-    if ((long long)need + lbv > best) return;
+    if ((long long)need + lbv > best) return false;
+  } else {
+    // full join: the answer at v is a tree rooted at v touching every group
+    for (int i = 0; i < k; ++i) {
+      int dm = INF;
+      for (int l = 0; l < L; ++l) dm = imin(dm, row[(1 + i) * L + l]);
+      dist[i] = clip_dist(dm, q.R1);
+    }
+    if (full_bound(dist, k, W, q.lbtab) > best) return false;
   }
   int M[LT > 0 ? LT : MAXL];
   merge_costs<LT>(row, sidx, S, L, D, M);
   if (s == k) {
     const int a = M[L - 1];
     if (a < INF) *ans = ((unsigned long long)(unsigned)a << 32) | (unsigned long long)v;
-    return;
+    return true;
   }
   for (int l = 0; l < L; ++l) {
     const int val = M[l];
@@ -536,13 +566,21 @@ __device__ __forceinline__ void merge_item(Slot& q, int t, uint32_t v, int r, in
     }
   }
   (void)t;
+  return true;
 }
 
-__global__ void __launch_bounds__(MERGE_THREADS)
+// 4 blocks per SM (64 registers, no spills): 25% faster than the 3 that 78
+// registers allow, on C2 and C4
+__global__ void __launch_bounds__(MERGE_THREADS, 4)
 k_merge(Slot* slots, const Plan* plan, Graph g) {
   __shared__ long long s_off[MAXSLOTS + 1];
   __shared__ int s_slot[MAXSLOTS];
   __shared__ uint8_t s_sidx[MAXK + 1][MAXW], s_sof[MAXK + 1][MAXW];
+  // per-thread singleton distances; the lower bound indexes them by set bit,
+  // which would put a register array in local memory.  An odd stride keeps
+  // the lanes of a warp in distinct banks.
+  __shared__ int s_dist[MERGE_THREADS * DIST_STRIDE];
+  int* dist = s_dist + threadIdx.x * DIST_STRIDE;
   const int nm = plan->n_merge;
   if (nm == 0) return;
   for (int x = threadIdx.x; x <= nm; x += blockDim.x) s_off[x] = plan->merge_off[x];
@@ -574,16 +612,17 @@ k_merge(Slot* slots, const Plan* plan, Graph g) {
       const uint8_t* sidx = s_sidx[k];
       v = q.touched[vi];
       key = ((unsigned long long)(unsigned)t << 32) | (unsigned)vi;
+      bool ev = false;
       switch (q.L) {
-        case 1: merge_item<1>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
-        case 2: merge_item<2>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
-        case 3: merge_item<3>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
-        case 4: merge_item<4>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
-        case 5: merge_item<5>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
-        case 6: merge_item<6>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
-        default: merge_item<0>(q, t, v, r, S, sidx, g, &ans, &dirty, &dmin); break;
+        case 1: ev = merge_item<1>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
+        case 2: ev = merge_item<2>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
+        case 3: ev = merge_item<3>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
+        case 4: ev = merge_item<4>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
+        case 5: ev = merge_item<5>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
+        case 6: ev = merge_item<6>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
+        default: ev = merge_item<0>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
       }
-      nsplit = (1ull << (__popc(S) - 1)) - 1;
+      if (ev) nsplit = (1ull << (__popc(S) - 1)) - 1;
     }
     // answers: one atomic per (warp, slot).  The segment reductions and heads
     // use full-warp shuffles, so every lane evaluates them unconditionally.
@@ -612,67 +651,114 @@ k_merge(Slot* slots, const Plan* plan, Graph g) {
   }
 }
 
+// Inclusive add-scan of x over lanes with equal key; segments must be runs of
+// consecutive lanes.  Every lane of the warp must call it.
+__device__ __forceinline__ int seg_iscan(int x, unsigned long long key) {
+  const int lane = threadIdx.x & 31;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    const unsigned long long ky = __shfl_up_sync(0xffffffffu, key, o);
+    if (lane >= o && ky == key) x += y;
+  }
+  return x;
+}
+
+// Reserves x consecutive entries of *counter per lane with one atomicAdd per
+// run of equal keys (the run's last lane adds the run's total and passes the
+// base on).  counter may differ between runs; lanes with x = 0 get an unused
+// position.  Every lane of the warp must call it.
+__device__ __forceinline__ int seg_reserve(int* counter, int x, unsigned long long key) {
+  const int incl = seg_iscan(x, key);
+  const unsigned run = __match_any_sync(0xffffffffu, key);
+  const int tail = 31 - __clz(run);
+  int base = 0;
+  if ((threadIdx.x & 31) == tail && incl > 0) base = atomicAdd(counter, incl);
+  base = __shfl_sync(0xffffffffu, base, tail);
+  return base + incl - x;
+}
+
 // ---------------------------------------------------------------------------
 // Prep: snapshot the dirty masks of this round's frontier and cut each
-// vertex's adjacency into chunks of bounded work.
+// vertex's adjacency into chunks of bounded work.  The far-list slots, chunk
+// ranges and frontier counts are reserved once per run of same-slot lanes.
 // ---------------------------------------------------------------------------
 __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
+  __shared__ long long s_off[MAXSLOTS + 1];
+  __shared__ int s_slot[MAXSLOTS];
   const int ng = plan->n_grow;
   if (ng == 0) return;
-  const long long total = plan->prep_off[ng];
-  for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < total;
+  for (int x = threadIdx.x; x <= ng; x += blockDim.x) s_off[x] = plan->prep_off[x];
+  for (int x = threadIdx.x; x < ng; x += blockDim.x) s_slot[x] = plan->grow_slots[x];
+  __syncthreads();
+  const long long total = s_off[ng];
+  const long long span = (total + 31) & ~31ll;  // whole warps: the reservations use shuffles
+  for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < span;
        gi += (long long)gridDim.x * blockDim.x) {
-    const int j = seg_search(plan->prep_off, ng, gi);
-    Slot& q = slots[plan->grow_slots[j]];
-    const bool hop = q.D >= 0;
-    const bool farround = !hop && q.farround;
-    const int lvl = hop ? q.d : 0;
-    const int qi = hop ? q.d : (farround ? (q.fcur ^ 1) : q.cur);
-    const uint32_t v = q.queue[(long long)qi * g.V + (gi - plan->prep_off[j])];
-    const long long plane = hop ? lvl : (farround ? 1 : 0);
-    unsigned long long m = atomicExch(&q.mask[plane * g.V + v], 0ull);
-    if (m == 0ull) continue;
-    {
-      // keep the sets whose cost is still a valid grow source (2 * cost <= best);
-      // plain problem: expand only costs below the bucket bound T and put the
-      // others back on the far list (cost order: a state is expanded once it
-      // is final rather than every time it improves)
-      const int best = *(volatile int*)&q.best;
-      const int k = q.k, L = q.L, lo = c_sub.loff[k][q.s];
-      const int T = hop ? INF : q.T;
-      const int32_t* src = q.table + (long long)v * q.W * L;
-      unsigned long long far = 0;
-      int fmin = INF;
-      for (unsigned long long x = m; x; x &= x - 1) {
-        const int r = __ffsll((long long)x) - 1;
-        const int sv = src[(lo + r) * L + lvl];
-        if (sv >= INF || 2LL * sv > best) {
-          m &= ~(1ull << r);
-        } else if (sv >= T) {
-          m &= ~(1ull << r);
-          far |= 1ull << r;
-          fmin = imin(fmin, sv);
+    int t = -1, nfar = 0, nch = 0, nb = 0, fmin = INF;
+    uint32_t v = 0;
+    unsigned long long m = 0;
+    long long eb = 0, ee = 0, ch = 1;
+    if (gi < total) {
+      const int j = seg_search(s_off, ng, gi);
+      t = s_slot[j];
+      Slot& q = slots[t];
+      const bool hop = q.D >= 0;
+      const bool farround = !hop && q.farround;
+      const int lvl = hop ? q.d : 0;
+      const int qi = hop ? q.d : (farround ? (q.fcur ^ 1) : q.cur);
+      v = q.queue[(long long)qi * g.V + (gi - s_off[j])];
+      const long long plane = hop ? lvl : (farround ? 1 : 0);
+      m = atomicExch(&q.mask[plane * g.V + v], 0ull);
+      if (m) {
+        // keep the sets whose cost is still a valid grow source (2 * cost <= best);
+        // plain problem: expand only costs below the bucket bound T and put the
+        // others back on the far list (cost order: a state is expanded once it
+        // is final rather than every time it improves)
+        const int best = *(volatile int*)&q.best;
+        const int k = q.k, L = q.L, lo = c_sub.loff[k][q.s];
+        const int T = hop ? INF : q.T;
+        const int32_t* src = q.table + (long long)v * q.W * L;
+        unsigned long long far = 0;
+        for (unsigned long long x = m; x; x &= x - 1) {
+          const int r = __ffsll((long long)x) - 1;
+          const int sv = src[(lo + r) * L + lvl];
+          if (sv >= INF || 2LL * sv > best) {
+            m &= ~(1ull << r);
+          } else if (sv >= T) {
+            m &= ~(1ull << r);
+            far |= 1ull << r;
+            fmin = imin(fmin, sv);
+          }
         }
-      }
-      if (far) {
-        const unsigned long long om = atomicOr(&q.mask[g.V + v], far);
-        if (om == 0ull) {
-          const int pos = atomicAdd(&q.qcount[q.fcur], 1);
-          if (pos < g.V) q.queue[(long long)q.fcur * g.V + pos] = v;
-          else q.err = ERR_QUEUE_CAP;
+        if (far) {
+          if (atomicOr(&q.mask[g.V + v], far) == 0ull) nfar = 1;
+          if (fmin < *(volatile int*)&q.next_min) atomicMin(&q.next_min, fmin);
         }
-        if (fmin < *(volatile int*)&q.next_min) atomicMin(&q.next_min, fmin);
+        if (m) {
+          eb = g.rowptr[v];
+          ee = g.rowptr[v + 1];
+          nb = __popcll(m);
+          if (ee > eb) {
+            ch = imax(32, 1024 / nb);
+            nch = (int)((ee - eb + ch - 1) / ch);
+          }
+        }
       }
     }
-    if (m == 0ull) continue;
-    const long long eb = g.rowptr[v], ee = g.rowptr[v + 1];
-    const int nb = __popcll(m);
-    atomicAdd(&q.st_frontier, (unsigned long long)nb);
-    if (ee == eb) continue;
-    const long long ch = imax(32, 1024 / nb);
-    const int nch = (int)((ee - eb + ch - 1) / ch);
-    const int pos = atomicAdd(&q.nchunks, nch);
-    if (pos + nch > q.chunk_cap) { q.err = ERR_CHUNK_CAP; continue; }
+    const unsigned long long key = t < 0 ? ~0ull : (unsigned long long)t;
+    Slot* qp = t < 0 ? slots : &slots[t];  // lanes past the end reserve nothing
+    const int fpos = seg_reserve(&qp->qcount[t < 0 ? 0 : qp->fcur], nfar, key);
+    const int cpos = seg_reserve(&qp->nchunks, nch, key);
+    const unsigned long long nfr = seg_add_u64((unsigned long long)nb, key);
+    if (t < 0) continue;
+    Slot& q = *qp;
+    if (seg_head(key) && nfr) atomicAdd(&q.st_frontier, nfr);
+    if (nfar) {
+      if (fpos < g.V) q.queue[(long long)q.fcur * g.V + fpos] = v;
+      else q.err = ERR_QUEUE_CAP;
+    }
+    if (nch == 0) continue;
+    if (cpos + nch > q.chunk_cap) { q.err = ERR_CHUNK_CAP; continue; }
     for (int c = 0; c < nch; ++c) {
       Chunk x;
       x.v = v;
@@ -680,7 +766,7 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
       x.ee = (uint32_t)(eb + (c + 1) * ch < ee ? eb + (c + 1) * ch : ee);
       x.pad = 0;
       x.mask = m;
-      q.chunks[pos + c] = x;
+      q.chunks[cpos + c] = x;
     }
   }
 }
@@ -692,7 +778,12 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
 // evaluated for candidates that improve it.
 // ---------------------------------------------------------------------------
 constexpr int GROW_WARPS = 8;
-constexpr int GROW_UNROLL = 4;
+// The grow is bound by the latency of dependent random reads, so resident
+// warps matter more than pairs in flight per lane: 6 blocks of 8 warps per SM
+// (40 registers, a few spills on the cold improvement path) with one pair per
+// lane beat 2 blocks with 4 pairs per lane by 25-35% on C2 and C4.
+constexpr int GROW_MIN_BLOCKS = 6;
+constexpr int GROW_UNROLL = 1;
 
 // Lower-bound test of a grow candidate (cold path: only improving candidates
 // reach it), kept out of line so the relaxation loop stays small.
@@ -749,7 +840,7 @@ __device__ __noinline__ void star_bound(Slot& q, const int32_t* trow, int k, int
   if (ub < *(volatile int*)&q.best) atomicMin(&q.best, (int)ub);
 }
 
-__global__ void __launch_bounds__(GROW_WARPS * 32, 2)
+__global__ void __launch_bounds__(GROW_WARPS * 32, GROW_MIN_BLOCKS)
 k_grow(Slot* slots, const Plan* plan, Graph g) {
   __shared__ long long s_off[MAXSLOTS + 1];
   __shared__ int s_slot[MAXSLOTS];

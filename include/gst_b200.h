@@ -135,7 +135,7 @@ typedef struct {
   int64_t frontier;     /* frontier states expanded (grow sources) */
   int64_t relax;        /* edge relaxations attempted */
   int64_t improve;      /* successful table updates (grow) */
-  int64_t merges;       /* merge partner pairs evaluated */
+  int64_t merges;       /* merge partner pairs evaluated (past the lower-bound pre-filter) */
   int64_t touched;      /* vertices that held a finite state */
   double device_ms;     /* device time from admission to answer */
 } gst_stats;
