@@ -86,6 +86,31 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def random_read_ceiling(torch, device) -> dict:
+    """Random 4-byte reads per second that a library gather reaches on this
+    GPU: torch.take of 64 Mi uniformly random int32 from a 4 GiB array (each
+    read costs at least a 32-byte sector).  It is the access pattern of the
+    grow kernel's target reads, so it bounds the grow better than the copy
+    bandwidth does."""
+    x = torch.empty(1 << 30, dtype=torch.int32, device=device)
+    x.fill_(1)
+    idx = torch.randint(0, 1 << 30, (64 << 20,), dtype=torch.int64, device=device)
+    out = torch.empty(64 << 20, dtype=torch.int32, device=device)
+    best = None
+    for _ in range(4):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        torch.take(x, idx, out=out)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        best = ms if best is None else min(best, ms)
+    del x, idx, out
+    torch.cuda.empty_cache()
+    return {"reads_per_s": (64 << 20) / (best / 1e3), "sector_gbs": (64 << 20) * 32 / (best / 1e3) / 1e9,
+            "how": "torch.take: 64 Mi random int32 reads from a 4 GiB array, best of 4"}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -357,6 +382,7 @@ def main():
     filter_queries(wl, args)
     queries = [q for q, _ in wl.queries]
     Ds = [D for _, D in wl.queries]
+    ceiling = random_read_ceiling(torch, f"cuda:{local}")  # before the engine takes its arena
     eng = gst_b200.Engine(device=local, profile=True, arena_bytes=int(args.arena_gb * (1 << 30)),
                           max_slots=args.max_slots, rounds_per_poll=args.rounds_per_poll,
                           bucket_shift=args.bucket_shift)
@@ -424,6 +450,7 @@ def main():
     single_qps = nsingle / (single_ms / 1e3) if single_ms > 0 else None
 
     peak, peak_kind = peaks()
+    grow_reads = sums["relax"] / (grow_ms / 1e3) if grow_ms > 0 else None
     gb = grow_bytes(sums)
     achieved = gb / (grow_ms / 1e3) / 1e9 if grow_ms > 0 else None
     traffic = None
@@ -456,7 +483,12 @@ def main():
                      "algorithmic_bytes_per_launch": gb / max(grow_launches, 1),
                      "avg_launch_ms": grow_ms / max(grow_launches, 1),
                      "grow_share_of_device_time": grow_ms / (tot_dev * 1e3) if tot_dev else None,
-                     "merge_ms": merge_ms},
+                     "merge_ms": merge_ms,
+                     # the grow's target reads are random 4-byte reads: their
+                     # rate against a library random gather on the same GPU
+                     "random_reads": {"grow_target_reads_per_s": grow_reads,
+                                      "ceiling": ceiling,
+                                      "frac": grow_reads / ceiling["reads_per_s"] if grow_reads else None}},
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -13,6 +13,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -101,6 +102,7 @@ struct Slab {
   uint32_t* queue = nullptr;
   uint32_t* touched = nullptr;
   uint32_t* tflag = nullptr;
+  uint32_t* dead = nullptr;
   Chunk* chunks = nullptr;
   int32_t* lbtab = nullptr;
   int32_t* wstack = nullptr;
@@ -152,6 +154,7 @@ class Engine {
     profile_ = c.profile != 0;
     bucket_shift_ = c.bucket_shift > 0 ? std::min(c.bucket_shift, 30) : 30;
     rounds_per_poll_ = c.rounds_per_poll > 0 ? c.rounds_per_poll : 8;
+    if (const char* w = std::getenv("GST_WATCHDOG_S")) watchdog_s_ = std::max(1.0, std::atof(w));
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
       return fail(GST_E_CUDA, "no CUDA device visible");
@@ -190,6 +193,10 @@ class Engine {
 
   void shutdown() {
     if (device_ < 0) return;
+    if (broken_) {  // device work still running: freeing would block on it
+      device_ = -1;
+      return;
+    }
     cudaSetDevice(device_);
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     graph_exec_ = nullptr;
@@ -325,6 +332,7 @@ class Engine {
   gst_status run(std::vector<std::shared_ptr<Request>>& reqs) {
     std::lock_guard<std::mutex> lk(mu_);
     if (busy_) return fail(GST_E_STATE, "engine is serving; use the server API");
+    if (broken_) return fail(GST_E_STATE, "engine is unusable after a device wait timed out");
     GST_CUDA(cudaSetDevice(device_));
     if (!ev_run0_) {
       GST_CUDA(cudaEventCreate(&ev_run0_));
@@ -414,6 +422,7 @@ class Engine {
     size_t o_queue = take(nq * V * 4);
     size_t o_touched = take(V * 4);
     size_t o_tflag = take(V * 4);
+    size_t o_dead = take((V + 31) / 32 * 4);
     size_t o_chunks = take((size_t)s.chunk_cap * sizeof(Chunk));
     size_t o_lbtab = take((size_t)sh.k * sh.k * W * 4 + (size_t)sh.k * W * 4);
     size_t o_wstack = take((size_t)s.wcap * 16);
@@ -427,6 +436,7 @@ class Engine {
       out->queue = reinterpret_cast<uint32_t*>(o_queue);
       out->touched = reinterpret_cast<uint32_t*>(o_touched);
       out->tflag = reinterpret_cast<uint32_t*>(o_tflag);
+      out->dead = reinterpret_cast<uint32_t*>(o_dead);
       out->chunks = reinterpret_cast<Chunk*>(o_chunks);
       out->lbtab = reinterpret_cast<int32_t*>(o_lbtab);
       out->wstack = reinterpret_cast<int32_t*>(o_wstack);
@@ -488,6 +498,7 @@ class Engine {
     place(s.queue);
     place(s.touched);
     place(s.tflag);
+    place(s.dead);
     place(s.chunks);
     place(s.lbtab);
     place(s.wstack);
@@ -497,12 +508,36 @@ class Engine {
     const size_t V = (size_t)V_, W = (size_t)1 << sh.k, L = (size_t)sh.L;
     if (cudaMemsetAsync(s.table, 0x3f, V * W * L * 4, stream_) != cudaSuccess ||
         cudaMemsetAsync(s.mask, 0, (sh.L == 1 ? 2 : L) * V * 8, stream_) != cudaSuccess ||
-        cudaMemsetAsync(s.tflag, 0, V * 4, stream_) != cudaSuccess) {
+        cudaMemsetAsync(s.tflag, 0, V * 4, stream_) != cudaSuccess ||
+        cudaMemsetAsync(s.dead, 0, (V + 31) / 32 * 4, stream_) != cudaSuccess) {
       arena_alloc_.release(off, bytes);
       return false;
     }
     *out = s;
     return true;
+  }
+
+  // Waits for the engine stream with a deadline.  A round sequence that does
+  // not finish within watchdog_s_ seconds (far above any legitimate poll
+  // interval) turns into GST_E_CUDA instead of blocking the caller for good;
+  // the engine is then unusable and the process should exit, which ends the
+  // device work with its context.
+  gst_status wait_stream() {
+    if (!ev_poll_) GST_CUDA(cudaEventCreateWithFlags(&ev_poll_, cudaEventDisableTiming));
+    GST_CUDA(cudaEventRecord(ev_poll_, stream_));
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int spin = 0;; ++spin) {
+      const cudaError_t q = cudaEventQuery(ev_poll_);
+      if (q == cudaSuccess) return GST_OK;
+      if (q != cudaErrorNotReady) return fail(GST_E_CUDA, std::string("engine stream: ") + cudaGetErrorString(q));
+      if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > watchdog_s_) {
+        broken_ = true;
+        return fail(GST_E_CUDA, "engine stream did not finish within " + std::to_string((int)watchdog_s_) +
+                                    " s (GST_WATCHDOG_S); the engine is unusable");
+      }
+      if (spin > 2000) std::this_thread::sleep_for(std::chrono::microseconds(100));
+      else std::this_thread::yield();
+    }
   }
 
   gst_status admit() {
@@ -532,10 +567,14 @@ class Engine {
       q.queue = sb.queue;
       q.touched = sb.touched;
       q.tflag = sb.tflag;
+      q.dead = sb.dead;
       q.chunks = sb.chunks;
       q.lbtab = sb.lbtab;
       q.wstack = sb.wstack;
       q.wedges = sb.wedges;
+      // merge lists borrow the witness stack (>= 8 V bytes, used only after the last merge)
+      q.live[0] = reinterpret_cast<uint32_t*>(sb.wstack);
+      q.live[1] = q.live[0] + V_;
       q.chunk_cap = sb.chunk_cap;
       q.wcap = sb.wcap;
       q.k = k;
@@ -625,7 +664,7 @@ class Engine {
     k_publish<<<(max_slots_ + 255) / 256, 256, 0, stream_>>>(d_slots_, max_slots_, d_status_);
     GST_CUDA(cudaMemcpyAsync(h_status_, d_status_, sizeof(SlotStatus) * max_slots_,
                              cudaMemcpyDeviceToHost, stream_));
-    GST_CUDA(cudaStreamSynchronize(stream_));
+    if (gst_status st = wait_stream(); st != GST_OK) return st;
     prof_.rounds += rounds_per_poll_;
     prof_.kernel_launches += 6 * rounds_per_poll_ + 1;
     prof_.d2h_bytes += sizeof(SlotStatus) * max_slots_;
@@ -772,6 +811,9 @@ class Engine {
   bool profile_ = false;
   std::vector<cudaEvent_t> ev_prof_;
   cudaEvent_t ev_run0_ = nullptr, ev_run1_ = nullptr;
+  cudaEvent_t ev_poll_ = nullptr;
+  double watchdog_s_ = 120.0;
+  bool broken_ = false;  // a device wait timed out: refuse further work
   gst_profile prof_{};
 };
 

@@ -16,6 +16,11 @@
 //   queue[qi][v]          frontier vertex lists (plain: near lists 0/1 and far
 //                          lists 2/3, ping-pong; D-: one list per depth label).
 //   touched[], tflag[v]   vertices that ever held a finite entry.
+//   dead[V / 32]          vertices the liveness test dropped (bitmap).
+//   live[2][V]            merge lists: the vertices a layer's merge visits;
+//                          each merge writes, for the next layer, the vertices
+//                          whose whole-tree lower bound is still <= best
+//                          (the witness stack's memory, idle until the end).
 //   chunks[]              the current round's grow work: (v, edge range, mask).
 //
 // INF = 0x3f3f3f3f so that a byte memset initialises a table and the sum of
@@ -92,6 +97,15 @@ struct Slot {
   // marks a round that drains the previous far list
   int32_t delta, bshift, T, next_min, fcur, farround;
   int32_t qcount[MAXQ];
+  // merge lists: layer s visits live[lr][0, nlr) and touched[mt0, mt1) (the
+  // vertices first touched since the previous list was cut) and appends the
+  // vertices that stay alive to live[lr ^ 1] (nlw entries)
+  uint32_t* live[2];
+  int32_t lr, nlr, nlw, mt0, mt1;
+  // dead[v >> 5] bit v & 31: the merge's liveness test dropped v (plain
+  // queries); grows and preps skip such vertices while use_dead is set
+  uint32_t* dead;
+  int32_t use_dead;
   unsigned long long answer;  // (cost << 32) | root
   unsigned long long st_frontier, st_relax, st_improve, st_merges;
 };

@@ -260,9 +260,29 @@ __global__ void k_ctl_a(Slot* slots, int nslots, Plan* plan, SlotStatus* status)
               act = (q.s == q.k) ? A_MERGEFULL : A_MERGE;
             }
           }
-          if (act == A_MERGE || act == A_MERGEFULL)  // one item per (touched vertex, set of the layer)
-            n_merge = (long long)q.ntouched * (c_sub.loff[q.k][q.s + 1] - c_sub.loff[q.k][q.s]);
+          if (act == A_MERGE || act == A_MERGEFULL) {
+            // one item per (listed vertex, set of the layer): the previous
+            // merge's live list plus the vertices touched since it was cut
+            if (q.s == 2 || hop) {
+              // D-queries visit every touched vertex: their best is rarely
+              // finite early enough for the liveness test to drop any
+              q.lr = 0;
+              q.nlr = 0;
+              q.mt0 = 0;
+            } else {
+              q.lr ^= 1;
+              q.nlr = q.nlw;
+              q.mt0 = q.mt1;
+            }
+            q.nlw = 0;
+            q.mt1 = q.ntouched;
+            n_merge = (long long)(q.nlr + q.mt1 - q.mt0) * (c_sub.loff[q.k][q.s + 1] - c_sub.loff[q.k][q.s]);
+          }
           if (act == A_GROW) n_prep = hop ? q.qcount[q.d] : q.qcount[q.farround ? (q.fcur ^ 1) : q.cur];
+          // plain layers >= 2: consult the dead bitmap in prep and grow once
+          // the last merge dropped most of the vertices it visited (the
+          // bitmap read is an extra dependent step for live targets)
+          q.use_dead = !hop && q.s >= 2 && 2LL * q.nlw < (long long)q.nlr + q.mt1 - q.mt0;
         }
       }
       q.action = act;
@@ -446,6 +466,46 @@ __device__ __forceinline__ bool seg_head(unsigned long long key) {
   return lane == 0 || pk != key;
 }
 
+// Inclusive add-scan of x over lanes with equal key; segments must be runs of
+// consecutive lanes.  Every lane of the warp must call it.
+__device__ __forceinline__ int seg_iscan(int x, unsigned long long key) {
+  const int lane = threadIdx.x & 31;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    const unsigned long long ky = __shfl_up_sync(0xffffffffu, key, o);
+    if (lane >= o && ky == key) x += y;
+  }
+  return x;
+}
+
+// Reserves x consecutive entries of *counter per lane with one atomicAdd per
+// run of equal keys (the run's last lane adds the run's total and passes the
+// base on).  counter may differ between runs; lanes with x = 0 get an unused
+// position.  Every lane of the warp must call it.  A warp with nothing to
+// reserve returns after one vote; a warp of one key scans without keys.
+__device__ __forceinline__ int seg_reserve(int* counter, int x, unsigned long long key) {
+  if (!__any_sync(0xffffffffu, x != 0)) return 0;
+  const int lane = threadIdx.x & 31;
+  const unsigned long long kf = __shfl_sync(0xffffffffu, key, 0), kl = __shfl_sync(0xffffffffu, key, 31);
+  int incl, tail;
+  if (kf == kl) {
+    incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    tail = 31;
+  } else {
+    incl = seg_iscan(x, key);
+    tail = 31 - __clz(__match_any_sync(0xffffffffu, key));
+  }
+  int base = 0;
+  if (lane == tail && incl > 0) base = atomicAdd(counter, incl);
+  base = __shfl_sync(0xffffffffu, base, tail);
+  return base + incl - x;
+}
+
 // Merged costs M[0..L) (prefix minima over labels) of set S at a vertex row.
 // sidx: the subset -> index map of this k (in shared memory: lanes look up
 // different subsets, which the constant cache would serialise).  With a
@@ -600,6 +660,7 @@ k_merge(Slot* slots, const Plan* plan, Graph g) {
     int t = -1;
     uint32_t v = 0;
     unsigned long long nsplit = 0;
+    int alive = 0;
     if (gi < total) {
       const int j = seg_search(s_off, nm, gi);
       t = s_slot[j];
@@ -610,7 +671,7 @@ k_merge(Slot* slots, const Plan* plan, Graph g) {
       const int vi = (int)(local / nS), r = (int)(local % nS);
       const int S = s_sof[k][lo + r];
       const uint8_t* sidx = s_sidx[k];
-      v = q.touched[vi];
+      v = vi < q.nlr ? q.live[q.lr][vi] : q.touched[q.mt0 + vi - q.nlr];
       key = ((unsigned long long)(unsigned)t << 32) | (unsigned)vi;
       bool ev = false;
       switch (q.L) {
@@ -623,58 +684,72 @@ k_merge(Slot* slots, const Plan* plan, Graph g) {
         default: ev = merge_item<0>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
       }
       if (ev) nsplit = (1ull << (__popc(S) - 1)) - 1;
+      // the vertex stays on the next layer's list while a tree through it
+      // can still cost <= best (best only falls, so a dropped vertex never
+      // returns); dist holds its singleton distances (computed for s < k)
+      if (r == 0 && s < k && q.D < 0) {
+        alive = full_bound(dist, k, q.W, q.lbtab) <= *(volatile int*)&q.best;
+        if (!alive) atomicOr(&q.dead[v >> 5], 1u << (v & 31));
+      }
     }
-    // answers: one atomic per (warp, slot).  The segment reductions and heads
-    // use full-warp shuffles, so every lane evaluates them unconditionally.
+    // Warp epilogue.  The segment reductions and heads use full-warp
+    // shuffles, so every lane evaluates them; each is skipped after one vote
+    // when no lane of the warp has anything to contribute.
     const unsigned long long skey = t < 0 ? ~0ull : (unsigned long long)(unsigned)t;
-    const unsigned long long amin = seg_min_u64(ans, skey);
-    const bool shead = seg_head(skey);
-    const bool vhead = seg_head(key);
-    if (t >= 0 && shead && amin != ~0ull) atomicMin(&slots[t].answer, amin);
+    // answers (full join only): one atomicMin per (warp, slot)
+    if (__any_sync(0xffffffffu, ans != ~0ull)) {
+      const unsigned long long amin = seg_min_u64(ans, skey);
+      const bool shead = seg_head(skey);  // every lane: a full-warp shuffle
+      if (t >= 0 && shead && amin != ~0ull) atomicMin(&slots[t].answer, amin);
+    }
     // plain seeds: one atomicOr (and at most one enqueue) per (warp, vertex),
     // into the far plane; the next grow round opens the first bucket at the
     // cheapest seed
-    const unsigned long long dor = seg_or_u64(dirty, key);
-    const unsigned long long dm = seg_min_u64((unsigned long long)(unsigned)dmin, key);
-    if (t >= 0 && vhead && dor) {
-      Slot& q = slots[t];
-      const unsigned long long om = atomicOr(&q.mask[g.V + v], dor);
-      if (om == 0ull) {
-        const int pos = atomicAdd(&q.qcount[q.fcur], 1);
-        if (pos < g.V) q.queue[(long long)q.fcur * g.V + pos] = v;
-        else q.err = ERR_QUEUE_CAP;
+    if (__any_sync(0xffffffffu, dirty != 0ull)) {
+      const bool vhead = seg_head(key);
+      const unsigned long long dor = seg_or_u64(dirty, key);
+      const unsigned long long dm = seg_min_u64((unsigned long long)(unsigned)dmin, key);
+      if (t >= 0 && vhead && dor) {
+        Slot& q = slots[t];
+        const unsigned long long om = atomicOr(&q.mask[g.V + v], dor);
+        if (om == 0ull) {
+          const int pos = atomicAdd(&q.qcount[q.fcur], 1);
+          if (pos < g.V) q.queue[(long long)q.fcur * g.V + pos] = v;
+          else q.err = ERR_QUEUE_CAP;
+        }
+        if ((int)dm < *(volatile int*)&q.next_min) atomicMin(&q.next_min, (int)dm);
       }
-      if ((int)dm < *(volatile int*)&q.next_min) atomicMin(&q.next_min, (int)dm);
     }
-    const unsigned long long ns = seg_add_u64(nsplit, skey);
-    if (t >= 0 && shead && ns) atomicAdd(&slots[t].st_merges, ns);
+    // split counter (statistics): a plain warp sum when the warp is one slot
+    {
+      const int tf = __shfl_sync(0xffffffffu, t, 0), tl = __shfl_sync(0xffffffffu, t, 31);
+      if (tf == tl && tf >= 0) {
+        const unsigned ns = __reduce_add_sync(0xffffffffu, (unsigned)nsplit);
+        if ((threadIdx.x & 31) == 0 && ns) atomicAdd(&slots[tf].st_merges, (unsigned long long)ns);
+      } else {
+        const unsigned long long ns = seg_add_u64(nsplit, skey);
+        const bool shead = seg_head(skey);  // every lane: a full-warp shuffle
+        if (t >= 0 && shead && ns) atomicAdd(&slots[t].st_merges, ns);
+      }
+    }
+    // live-list append: one vertex per nS items appends, so most warps skip
+    // this after one vote; the alive lanes of one slot share one atomicAdd
+    const unsigned am = __ballot_sync(0xffffffffu, alive);
+    if (am) {
+      const int lane = threadIdx.x & 31;
+      const int l0 = __ffs(am) - 1, l1 = 31 - __clz(am);
+      const int t0 = __shfl_sync(0xffffffffu, t, l0), t1 = __shfl_sync(0xffffffffu, t, l1);
+      if (t0 == t1) {
+        int base = 0;
+        if (lane == l0) base = atomicAdd(&slots[t0].nlw, __popc(am));
+        base = __shfl_sync(0xffffffffu, base, l0);
+        if (alive) slots[t].live[slots[t].lr ^ 1][base + __popc(am & ((1u << lane) - 1))] = v;
+      } else if (alive) {
+        const int pos = atomicAdd(&slots[t].nlw, 1);
+        slots[t].live[slots[t].lr ^ 1][pos] = v;
+      }
+    }
   }
-}
-
-// Inclusive add-scan of x over lanes with equal key; segments must be runs of
-// consecutive lanes.  Every lane of the warp must call it.
-__device__ __forceinline__ int seg_iscan(int x, unsigned long long key) {
-  const int lane = threadIdx.x & 31;
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    const unsigned long long ky = __shfl_up_sync(0xffffffffu, key, o);
-    if (lane >= o && ky == key) x += y;
-  }
-  return x;
-}
-
-// Reserves x consecutive entries of *counter per lane with one atomicAdd per
-// run of equal keys (the run's last lane adds the run's total and passes the
-// base on).  counter may differ between runs; lanes with x = 0 get an unused
-// position.  Every lane of the warp must call it.
-__device__ __forceinline__ int seg_reserve(int* counter, int x, unsigned long long key) {
-  const int incl = seg_iscan(x, key);
-  const unsigned run = __match_any_sync(0xffffffffu, key);
-  const int tail = 31 - __clz(run);
-  int base = 0;
-  if ((threadIdx.x & 31) == tail && incl > 0) base = atomicAdd(counter, incl);
-  base = __shfl_sync(0xffffffffu, base, tail);
-  return base + incl - x;
 }
 
 // ---------------------------------------------------------------------------
@@ -709,6 +784,7 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
       v = q.queue[(long long)qi * g.V + (gi - s_off[j])];
       const long long plane = hop ? lvl : (farround ? 1 : 0);
       m = atomicExch(&q.mask[plane * g.V + v], 0ull);
+      if (m && q.use_dead && ((q.dead[v >> 5] >> (v & 31)) & 1u)) m = 0;  // no optimal tree reaches v
       if (m) {
         // keep the sets whose cost is still a valid grow source (2 * cost <= best);
         // plain problem: expand only costs below the bucket bound T and put the
@@ -750,9 +826,10 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
     const int fpos = seg_reserve(&qp->qcount[t < 0 ? 0 : qp->fcur], nfar, key);
     const int cpos = seg_reserve(&qp->nchunks, nch, key);
     const unsigned long long nfr = seg_add_u64((unsigned long long)nb, key);
+    const bool head = seg_head(key);  // every lane: a full-warp shuffle
     if (t < 0) continue;
     Slot& q = *qp;
-    if (seg_head(key) && nfr) atomicAdd(&q.st_frontier, nfr);
+    if (head && nfr) atomicAdd(&q.st_frontier, nfr);
     if (nfar) {
       if (fpos < g.V) q.queue[(long long)q.fcur * g.V + fpos] = v;
       else q.err = ERR_QUEUE_CAP;
@@ -779,17 +856,18 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
 // ---------------------------------------------------------------------------
 constexpr int GROW_WARPS = 8;
 // The grow is bound by the latency of dependent random reads, so resident
-// warps matter more than pairs in flight per lane: 6 blocks of 8 warps per SM
-// (40 registers, a few spills on the cold improvement path) with one pair per
-// lane beat 2 blocks with 4 pairs per lane by 25-35% on C2 and C4.
-constexpr int GROW_MIN_BLOCKS = 6;
-constexpr int GROW_UNROLL = 1;
+// warps matter more than pairs in flight per lane.  With no call in the
+// relaxation loop it needs 64 registers: 4 blocks of 8 warps per SM
+// (measured best; 6 blocks at 40 registers spill onto the loop).
+constexpr int GROW_MIN_BLOCKS = 4;
+constexpr int GROW_QUEUE = 128;  // improving candidates queued per warp
 
 // Lower-bound test of a grow candidate (cold path: only improving candidates
 // reach it), kept out of line so the relaxation loop stays small.
-__device__ __noinline__ bool lb_prunes(const int32_t* trow, int k, int W, int L, int S, int R1,
-                                       const int32_t* lbtab, int nc, int best) {
-  int dist[MAXK];
+// dist: a per-thread scratch of k ints (shared memory: the bound indexes it
+// by set bit, which would put a register array in local memory).
+__device__ __forceinline__ bool lb_prunes(const int32_t* trow, int k, int W, int L, int S, int R1,
+                                          const int32_t* lbtab, int nc, int best, int* dist) {
   for (int i = 0; i < k; ++i) {
     int dm = INF;
     for (int l = 0; l < L; ++l) dm = imin(dm, trow[(1 + i) * L + l]);
@@ -816,7 +894,7 @@ __device__ __forceinline__ void flush_counts(Slot& q, unsigned long long& nrel, 
 // cheapest path to every group, joined at the vertex.  With a diameter bound D
 // every branch may be hl = floor(D/2) hops deep and one of them hh = ceil(D/2)
 // (any two branches then span at most D hops).
-__device__ __noinline__ void star_bound(Slot& q, const int32_t* trow, int k, int L, int hl, int hh) {
+__device__ __forceinline__ void star_bound(Slot& q, const int32_t* trow, int k, int L, int hl, int hh) {
   long long sum = 0, gain = 0;
   int ninf = 0;
   long long deep_only = INF;  // the one group reachable only within hh hops
@@ -840,12 +918,43 @@ __device__ __noinline__ void star_bound(Slot& q, const int32_t* trow, int k, int
   if (ub < *(volatile int*)&q.best) atomicMin(&q.best, (int)ub);
 }
 
+// Cold path of a relaxation: candidate cost nc beats the target entry
+// (u, rank rS & 0xff, label td) read a moment ago; rS >> 8 is the subset.
+// Runs between relaxation batches, inline (a call's register convention
+// would cost the relaxation loop occupancy).  Returns 1 for an improvement
+// that survives the lower-bound test.
+__device__ __forceinline__ int grow_improve(Slot& q, long long V, uint32_t u, int rS, int nc, int td, int* dist) {
+  const int k = q.k, W = q.W, L = q.L, D = q.D, s = q.s, r = rS & 0xff;
+  const bool hop = D >= 0;
+  const int best = *(volatile int*)&q.best;  // may be newer than the chunk's: only tighter
+  int32_t* trow = q.table + (long long)u * (W * L);
+  const long long tidx = (long long)(c_sub.loff[k][s] + r) * L;
+  // A candidate that fails the lower-bound test is still a real derivation
+  // cost: store it (unmarked, so never grown from) so that later, costlier
+  // candidates for this state stop at the plain read instead of re-running
+  // the bound.
+  const bool pruned = s >= 2 && lb_prunes(trow, k, W, L, rS >> 8, q.R1, q.lbtab, nc, best, dist);
+  const int old = atomicMin(&trow[tidx + td], nc);
+  if (old <= nc) return 0;
+  touch(q, u);
+  if (pruned) return 0;
+  if (s == 1 && (!hop || td <= (D + 1) / 2)) star_bound(q, trow, k, L, hop ? D / 2 : 0, hop ? (D + 1) / 2 : 0);
+  if (2LL * nc <= best) {
+    if (!hop) mark_plain(q, V, u, r, nc);
+    else if (td < D) mark_dirty(q, V, u, r, td, td);
+  }
+  return 1;
+}
+
 __global__ void __launch_bounds__(GROW_WARPS * 32, GROW_MIN_BLOCKS)
 k_grow(Slot* slots, const Plan* plan, Graph g) {
   __shared__ long long s_off[MAXSLOTS + 1];
   __shared__ int s_slot[MAXSLOTS];
   __shared__ int s_r[GROW_WARPS][64];
   __shared__ int s_sv[GROW_WARPS][64];
+  __shared__ int s_qu[GROW_WARPS][GROW_QUEUE], s_qr[GROW_WARPS][GROW_QUEUE], s_qc[GROW_WARPS][GROW_QUEUE];
+  __shared__ int s_dist[GROW_WARPS * 32 * DIST_STRIDE];
+  int* dist = s_dist + threadIdx.x * DIST_STRIDE;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int ng = plan->n_grow;
@@ -865,12 +974,12 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
     }
     Slot& q = slots[s_slot[j]];
     const Chunk c = q.chunks[gi - s_off[j]];
-    const int k = q.k, W = q.W, L = q.L, rowlen = W * L, D = q.D, s = q.s;
-    const bool hop = D >= 0;
+    const int k = q.k, L = q.L, rowlen = q.W * L;
+    const bool hop = q.D >= 0;
     const int d = hop ? q.d : 0;
     const int td = hop ? d + 1 : 0;
-    const int best = *(volatile int*)&q.best;
-    const int lo = c_sub.loff[k][s];
+    const int lo = c_sub.loff[k][q.s];
+    const bool use_dead = q.use_dead;
     const int32_t* src = q.table + (long long)c.v * rowlen;
     // the chunk's dirty sets (filtered to valid grow sources by the prep pass)
     int nact = 0;
@@ -892,62 +1001,50 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
     __syncwarp();
     if (nact > 0) {
       const int npairs = (int)(c.ee - c.eb) * nact;
-      // pair p = (edge p / nact, set p % nact), advanced incrementally by 32;
-      // GROW_UNROLL pairs per lane are loaded before any is compared, so each
-      // lane keeps several neighbour and target reads in flight
+      // pair p0 + lane = (edge / nact, set % nact), advanced incrementally by
+      // 32.  The relaxation loop makes no calls (a call's register
+      // convention would cost it occupancy): candidates that beat their
+      // target are queued in shared memory and handled between batches.
       const int q32 = 32 / nact, r32 = 32 % nact;
       int e = (int)c.eb + lane / nact, bi = lane % nact;
-      for (int p = lane; p < npairs; p += 32 * GROW_UNROLL) {
-        int2 a[GROW_UNROLL];
-        int rr[GROW_UNROLL], nc[GROW_UNROLL], cur[GROW_UNROLL];
-#pragma unroll
-        for (int i = 0; i < GROW_UNROLL; ++i) {
-          nc[i] = INF;
-          rr[i] = 0;
-          if (p + 32 * i < npairs) {
-            a[i] = __ldg(&g.adj[e]);
-            rr[i] = s_r[wib][bi];
-            nc[i] = s_sv[wib][bi] + a[i].y;
+      int p0 = 0;
+      while (true) {
+        int nb = 0;  // queued candidates (warp-uniform)
+        for (; p0 < npairs && nb <= GROW_QUEUE - 32; p0 += 32) {
+          int nc = INF, rS = 0;
+          int2 a = make_int2(0, 0);
+          if (p0 + lane < npairs) {
+            a = __ldg(&g.adj[e]);
+            rS = s_r[wib][bi];
+            nc = s_sv[wib][bi] + a.y;
             ++nrel;
+            if (use_dead && ((q.dead[(uint32_t)a.x >> 5] >> (a.x & 31)) & 1u)) nc = INF;
           }
           e += q32;
           bi += r32;
           if (bi >= nact) { bi -= nact; ++e; }
-        }
-#pragma unroll
-        for (int i = 0; i < GROW_UNROLL; ++i) {
-          cur[i] = INF;
-          if (nc[i] < INF) {
-            const int32_t* trow = q.table + (long long)a[i].x * rowlen;
-            const long long tidx = (long long)(lo + (rr[i] & 0xff)) * L;
+          bool imp = false;
+          if (nc < INF) {
+            const int32_t* trow = q.table + (long long)a.x * rowlen;
+            const long long tidx = (long long)(lo + (rS & 0xff)) * L;
             int cv = trow[tidx + td];
             for (int l = 0; l < td; ++l) cv = imin(cv, trow[tidx + l]);
-            cur[i] = cv;
+            imp = nc < cv;
           }
-        }
-#pragma unroll
-        for (int i = 0; i < GROW_UNROLL; ++i) {
-          if (nc[i] >= cur[i]) continue;  // also skips pairs past the end (nc = INF)
-          const uint32_t u = (uint32_t)a[i].x;
-          const int r = rr[i] & 0xff;
-          int32_t* trow = q.table + (long long)u * rowlen;
-          const long long tidx = (long long)(lo + r) * L;
-          // A candidate that fails the lower-bound test is still a real
-          // derivation cost: store it (unmarked, so never grown from) so that
-          // later, costlier candidates for this state stop at the read above
-          // instead of re-running the bound.
-          const bool pruned = s >= 2 && lb_prunes(trow, k, W, L, rr[i] >> 8, q.R1, q.lbtab, nc[i], best);
-          const int old = atomicMin(&trow[tidx + td], nc[i]);
-          if (old <= nc[i]) continue;
-          touch(q, u);
-          if (pruned) continue;
-          ++nimp;
-          if (s == 1 && (!hop || td <= (D + 1) / 2)) star_bound(q, trow, k, L, hop ? D / 2 : 0, hop ? (D + 1) / 2 : 0);
-          if (2LL * nc[i] <= best) {
-            if (!hop) mark_plain(q, g.V, u, r, nc[i]);
-            else if (td < D) mark_dirty(q, g.V, u, r, td, td);
+          const unsigned im = __ballot_sync(0xffffffffu, imp);
+          if (imp) {
+            const int x = nb + __popc(im & ((1u << lane) - 1));
+            s_qu[wib][x] = a.x;
+            s_qr[wib][x] = rS;
+            s_qc[wib][x] = nc;
           }
+          nb += __popc(im);
         }
+        __syncwarp();
+        for (int x = lane; x < nb; x += 32)
+          nimp += grow_improve(q, g.V, (uint32_t)s_qu[wib][x], s_qr[wib][x], s_qc[wib][x], td, dist);
+        __syncwarp();
+        if (p0 >= npairs) break;
       }
     }
     __syncwarp();
@@ -1136,7 +1233,10 @@ __global__ void k_reset(Slot* slots, int t, Graph g) {
        x += (long long)gridDim.x * blockDim.x) {
     const uint32_t v = q.touched[x / planes];
     q.mask[(x % planes) * g.V + v] = 0ull;
-    if (x % planes == 0) q.tflag[v] = 0u;
+    if (x % planes == 0) {
+      q.tflag[v] = 0u;
+      q.dead[v >> 5] = 0u;  // only touched vertices are ever marked
+    }
   }
 }
 

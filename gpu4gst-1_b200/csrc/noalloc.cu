@@ -158,8 +158,10 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   const size_t o_queue = take(nq * (size_t)V * 4);
   const size_t o_touched = take((size_t)V * 4);
   const size_t o_tflag = take((size_t)V * 4);
+  const size_t o_dead = take(((size_t)V + 31) / 32 * 4);
   const size_t o_chunks = take(chunk_cap * sizeof(Chunk));
   const size_t o_lbtab = take((size_t)kk * kk * W * 4 + (size_t)kk * W * 4);
+  const size_t o_live = take(2 * (size_t)V * 4);
   if (off > kScratchBytes)
     return fail(GST_E_NOMEM, "noalloc: query needs " + std::to_string(off >> 20) + " MiB of scratch, above the " +
                                  std::to_string(kScratchBytes >> 20) + " MiB static maximum");
@@ -174,8 +176,11 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   q.queue = reinterpret_cast<uint32_t*>(base + o_queue);
   q.touched = reinterpret_cast<uint32_t*>(base + o_touched);
   q.tflag = reinterpret_cast<uint32_t*>(base + o_tflag);
+  q.dead = reinterpret_cast<uint32_t*>(base + o_dead);
   q.chunks = reinterpret_cast<Chunk*>(base + o_chunks);
   q.lbtab = reinterpret_cast<int32_t*>(base + o_lbtab);
+  q.live[0] = reinterpret_cast<uint32_t*>(base + o_live);
+  q.live[1] = q.live[0] + V;
   q.wstack = nullptr;
   q.wedges = nullptr;
   q.chunk_cap = (long long)chunk_cap;
@@ -202,6 +207,7 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   ce = cudaMemsetAsync(base + o_table, 0x3f, (size_t)V * W * L * 4, s);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_mask, 0, planes * (size_t)V * 8, s);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_tflag, 0, (size_t)V * 4, s);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_dead, 0, ((size_t)V + 31) / 32 * 4, s);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(d_plan, 0, sizeof(Plan), s);
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_slot, &q, sizeof q, cudaMemcpyHostToDevice, s);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);  // q lives on this stack frame

@@ -117,6 +117,11 @@ typedef struct {
                               (0 -> 30: the lightest-edge width, best measured) */
 } gst_engine_config;
 
+/* Device waits of an engine are bounded: if a poll of the round sequence does
+ * not complete within GST_WATCHDOG_S seconds (environment variable, default
+ * 120), the call returns GST_E_CUDA and the engine refuses further work; the
+ * process should then exit (which ends the device work with its context).
+ * gst_engine_destroy of such an engine frees nothing. */
 gst_status gst_engine_create(const gst_engine_config* cfg, gst_engine** out);
 void gst_engine_destroy(gst_engine* e);
 
