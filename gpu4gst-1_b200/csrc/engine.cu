@@ -180,7 +180,8 @@ class Engine {
     GST_CUDA(cudaMallocHost(&h_status_, sizeof(SlotStatus) * MAXSLOTS));
     GST_CUDA(cudaMalloc(&d_list_, sizeof(int) * MAXSLOTS));
     GST_CUDA(cudaMallocHost(&h_list_, sizeof(int) * MAXSLOTS));
-    GST_CUDA(cudaMallocHost(&h_slot_, sizeof(Slot)));
+    GST_CUDA(cudaMallocHost(&h_slot_, sizeof(Slot) * MAXSLOTS));  // admission staging, one per slot
+    GST_CUDA(cudaMallocHost(&h_harv_, sizeof(Slot) * MAXSLOTS));  // harvest read-back
     size_t fr = 0, tot = 0;
     GST_CUDA(cudaMemGetInfo(&fr, &tot));
     arena_request_ = c.arena_bytes > 0 ? (size_t)c.arena_bytes
@@ -203,7 +204,7 @@ class Engine {
     for (auto* p : {(void*)d_slots_, (void*)d_plan_, (void*)d_status_, (void*)d_list_, (void*)arena_,
                     (void*)d_rowptr_, (void*)d_adj_, (void*)d_gptr_, (void*)d_gmem_})
       if (p) cudaFree(p);
-    for (auto* p : {(void*)h_status_, (void*)h_list_, (void*)h_slot_})
+    for (auto* p : {(void*)h_status_, (void*)h_list_, (void*)h_slot_, (void*)h_harv_, (void*)h_wedges_})
       if (p) cudaFreeHost(p);
     if (stream_) cudaStreamDestroy(stream_);
     d_slots_ = nullptr;
@@ -560,7 +561,7 @@ class Engine {
         break;  // wait for running queries to free memory
       }
       pending_.pop_front();
-      Slot& q = *h_slot_;
+      Slot& q = h_slot_[t];  // its previous copy finished: the slot was harvested after a sync
       std::memset(&q, 0, sizeof q);
       q.table = sb.table;
       q.mask = sb.mask;
@@ -598,7 +599,6 @@ class Engine {
       q.fcur = 2;
       GST_CUDA(cudaMemcpyAsync(d_slots_ + t, &q, sizeof(Slot), cudaMemcpyHostToDevice, stream_));
       prof_.h2d_bytes += sizeof(Slot);
-      GST_CUDA(cudaStreamSynchronize(stream_));  // h_slot_ is reused
       if (!r->t0) GST_CUDA(cudaEventCreate(&r->t0));
       GST_CUDA(cudaEventRecord(r->t0, stream_));
       Graph g = graph();
@@ -705,12 +705,36 @@ class Engine {
       prof_.kernel_launches += 1;
       prof_.h2d_bytes += sizeof(int) * wit.size();
     }
-    for (int t : fin) {
+    // one read-back of the slot array, then one batch of tree-edge copies
+    GST_CUDA(cudaMemcpyAsync(h_harv_, d_slots_, sizeof(Slot) * nslots_hw_, cudaMemcpyDeviceToHost, stream_));
+    GST_CUDA(cudaStreamSynchronize(stream_));
+    prof_.d2h_bytes += sizeof(Slot) * nslots_hw_;
+    std::vector<size_t> woff(fin.size() + 1, 0);
+    for (size_t i = 0; i < fin.size(); ++i) {
+      const Slot& q = h_harv_[fin[i]];
+      const bool tree = q.phase == PH_DONE && q.err == ERR_NONE && (q.answer >> 32) < (unsigned long long)INF;
+      woff[i + 1] = woff[i] + (tree ? 3 * (size_t)q.nwedges : 0);
+    }
+    const size_t wtot = woff[fin.size()];
+    if (wtot > wedge_cap_) {
+      if (h_wedges_) cudaFreeHost(h_wedges_);
+      h_wedges_ = nullptr;
+      wedge_cap_ = 0;
+      const size_t cap = std::max(wtot, (size_t)1 << 16);
+      GST_CUDA(cudaMallocHost(&h_wedges_, sizeof(int32_t) * cap));
+      wedge_cap_ = cap;
+    }
+    for (size_t i = 0; i < fin.size(); ++i) {
+      const size_t n = woff[i + 1] - woff[i];
+      if (n) GST_CUDA(cudaMemcpyAsync(h_wedges_ + woff[i], h_harv_[fin[i]].wedges, sizeof(int32_t) * n,
+                                      cudaMemcpyDeviceToHost, stream_));
+      prof_.d2h_bytes += sizeof(int32_t) * n;
+    }
+    if (wtot) GST_CUDA(cudaStreamSynchronize(stream_));
+    for (size_t fi = 0; fi < fin.size(); ++fi) {
+      const int t = fin[fi];
       auto r = slot_req_[t];
-      GST_CUDA(cudaMemcpyAsync(h_slot_, d_slots_ + t, sizeof(Slot), cudaMemcpyDeviceToHost, stream_));
-      GST_CUDA(cudaStreamSynchronize(stream_));
-      prof_.d2h_bytes += sizeof(Slot);
-      Slot q = *h_slot_;
+      const Slot q = h_harv_[t];
       gst_result& res = r->result;
       std::memset(&res, 0, sizeof res);
       res.root = -1;
@@ -738,9 +762,7 @@ class Engine {
         res.feasible = 1;
         res.root = (int32_t)(q.answer & 0xffffffffu);
         const int ne = q.nwedges;
-        std::vector<int32_t> e(3 * (size_t)ne);
-        if (ne) GST_CUDA(cudaMemcpy(e.data(), q.wedges, sizeof(int32_t) * 3 * ne, cudaMemcpyDeviceToHost));
-        prof_.d2h_bytes += sizeof(int32_t) * 3 * ne;
+        const int32_t* e = h_wedges_ + woff[fi];
         // the derivation may list an edge twice; report each edge once
         std::set<std::pair<int, int>> seen;
         std::vector<int32_t> uniq;
@@ -760,11 +782,22 @@ class Engine {
         }
         r->status = GST_OK;
       }
-      // clean the slab for reuse and free the slot
-      k_reset<<<num_sms_ * 2, 256, 0, stream_>>>(d_slots_, t, g);
+      // clean the slab for reuse and free the slot: row by row when few
+      // vertices were touched, else plain memsets of the whole slab arrays
+      const Slab& sb = slot_slab_[t];
+      if ((int64_t)q.ntouched * 4 < V_) {
+        k_reset<<<num_sms_ * 2, 256, 0, stream_>>>(d_slots_, t, g);
+        prof_.kernel_launches += 1;
+      } else {
+        const size_t V = (size_t)V_, W = (size_t)1 << sb.shape.k, L = (size_t)sb.shape.L;
+        GST_CUDA(cudaMemsetAsync(sb.table, 0x3f, V * W * L * 4, stream_));
+        GST_CUDA(cudaMemsetAsync(sb.mask, 0, (L == 1 ? 2 : L) * V * 8, stream_));
+        GST_CUDA(cudaMemsetAsync(sb.tflag, 0, V * 4, stream_));
+        GST_CUDA(cudaMemsetAsync(sb.dead, 0, (V + 31) / 32 * 4, stream_));
+      }
       k_free_slot<<<1, 1, 0, stream_>>>(d_slots_, t);
       GST_CUDA(cudaGetLastError());
-      prof_.kernel_launches += 2;
+      prof_.kernel_launches += 1;
       cache_[slot_slab_[t].shape].push_back(slot_slab_[t]);
       slot_busy_[t] = 0;
       slot_req_[t] = nullptr;
@@ -789,6 +822,9 @@ class Engine {
   int* d_list_ = nullptr;
   int* h_list_ = nullptr;
   Slot* h_slot_ = nullptr;
+  Slot* h_harv_ = nullptr;
+  int32_t* h_wedges_ = nullptr;
+  size_t wedge_cap_ = 0;
   long long* d_rowptr_ = nullptr;
   int2* d_adj_ = nullptr;
   long long* d_gptr_ = nullptr;
