@@ -34,6 +34,18 @@ namespace gst {
 
 __constant__ SubsetTables c_sub;
 
+constexpr int GROW_WARPS = 8;
+// The grow is bound by the latency of dependent random reads, so resident
+// warps matter more than pairs in flight per lane.  With no call in the
+// relaxation loop it needs 64 registers: 4 blocks of 8 warps per SM
+// (measured best; 6 blocks at 40 registers spill onto the loop).
+constexpr int GROW_MIN_BLOCKS = 4;
+constexpr int GROW_QUEUE = 128;  // improving candidates queued per warp
+// Lanes per chunk: a warp relaxes 32 / GROW_LANES chunks side by side, so
+// the per-chunk latency (descriptor, source row, dirty sets) overlaps.
+constexpr int GROW_LANES = 16;
+constexpr int GROW_CPW = 32 / GROW_LANES;  // chunks per warp
+
 
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
@@ -341,6 +353,7 @@ __global__ void k_ctl_b(Slot* slots, Plan* plan) {
     Slot& q = slots[plan->grow_slots[t]];
     c = q.nchunks;
     if (c > q.chunk_cap) { q.err = ERR_CHUNK_CAP; c = 0; }
+    c = (c + GROW_CPW - 1) / GROW_CPW;  // grow units: GROW_CPW chunks each
   }
   s_scan[t] = c;
   __syncthreads();
@@ -849,18 +862,12 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
 }
 
 // ---------------------------------------------------------------------------
-// Grow: one warp per chunk.  Lanes walk (edge, dirty set) pairs with the set
-// index fastest, so the lanes relaxing one neighbour touch adjacent words of
-// its row.  A target is read before the atomicMin and the lower bound is only
+// Grow: one group of GROW_LANES lanes per chunk, 32 / GROW_LANES chunks of
+// one slot per warp.  Lanes walk (edge, dirty set) pairs with the set index
+// fastest, so the lanes relaxing one neighbour touch adjacent words of its
+// row.  A target is read before the atomicMin and the lower bound is only
 // evaluated for candidates that improve it.
 // ---------------------------------------------------------------------------
-constexpr int GROW_WARPS = 8;
-// The grow is bound by the latency of dependent random reads, so resident
-// warps matter more than pairs in flight per lane.  With no call in the
-// relaxation loop it needs 64 registers: 4 blocks of 8 warps per SM
-// (measured best; 6 blocks at 40 registers spill onto the loop).
-constexpr int GROW_MIN_BLOCKS = 4;
-constexpr int GROW_QUEUE = 128;  // improving candidates queued per warp
 
 // Lower-bound test of a grow candidate (cold path: only improving candidates
 // reach it), kept out of line so the relaxation loop stays small.
@@ -950,13 +957,15 @@ __global__ void __launch_bounds__(GROW_WARPS * 32, GROW_MIN_BLOCKS)
 k_grow(Slot* slots, const Plan* plan, Graph g) {
   __shared__ long long s_off[MAXSLOTS + 1];
   __shared__ int s_slot[MAXSLOTS];
-  __shared__ int s_r[GROW_WARPS][64];
-  __shared__ int s_sv[GROW_WARPS][64];
+  __shared__ int s_r[GROW_WARPS][GROW_CPW * 64];
+  __shared__ int s_sv[GROW_WARPS][GROW_CPW * 64];
   __shared__ int s_qu[GROW_WARPS][GROW_QUEUE], s_qr[GROW_WARPS][GROW_QUEUE], s_qc[GROW_WARPS][GROW_QUEUE];
   __shared__ int s_dist[GROW_WARPS * 32 * DIST_STRIDE];
   int* dist = s_dist + threadIdx.x * DIST_STRIDE;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
+  const int sub = lane / GROW_LANES, sl = lane % GROW_LANES;  // lane group and lane in it
+  const unsigned gmask = GROW_LANES == 32 ? 0xffffffffu : ((1u << GROW_LANES) - 1) << (sub * GROW_LANES);
   const int ng = plan->n_grow;
   if (ng == 0) return;
   for (int x = threadIdx.x; x <= ng; x += blockDim.x) s_off[x] = plan->chunk_off[x];
@@ -973,7 +982,11 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
       cur_slot = s_slot[j];
     }
     Slot& q = slots[s_slot[j]];
-    const Chunk c = q.chunks[gi - s_off[j]];
+    // this lane group's chunk of the unit (none past the slot's last chunk)
+    const long long ci = (gi - s_off[j]) * GROW_CPW + sub;
+    Chunk c;
+    c.v = 0; c.eb = 0; c.ee = 0; c.pad = 0; c.mask = 0ull;
+    if (ci < q.nchunks) c = q.chunks[ci];
     const int k = q.k, L = q.L, rowlen = q.W * L;
     const bool hop = q.D >= 0;
     const int d = hop ? q.d : 0;
@@ -981,48 +994,53 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
     const int lo = c_sub.loff[k][q.s];
     const bool use_dead = q.use_dead;
     const int32_t* src = q.table + (long long)c.v * rowlen;
+    int* gr = s_r[wib] + sub * 64;
+    int* gsv = s_sv[wib] + sub * 64;
     // the chunk's dirty sets (filtered to valid grow sources by the prep pass)
     int nact = 0;
-    for (int base = 0; base < 64; base += 32) {
-      const int b = base + lane;
+    for (int base = 0; base < 64; base += GROW_LANES) {
+      const int b = base + sl;
       int r = -1, sv = INF;
       if ((c.mask >> b) & 1ull) {
         r = b;
         sv = src[(lo + r) * L + d];
       }
-      const unsigned ok = __ballot_sync(0xffffffffu, r >= 0);
+      const unsigned ok = (__ballot_sync(0xffffffffu, r >= 0) & gmask) >> (sub * GROW_LANES);
       if (r >= 0) {
-        const int p = nact + __popc(ok & ((1u << lane) - 1));
-        s_r[wib][p] = (int)c_sub.sof[k][lo + r] << 8 | r;  // (subset, rank)
-        s_sv[wib][p] = sv;
+        const int p = nact + __popc(ok & ((1u << sl) - 1));
+        gr[p] = (int)c_sub.sof[k][lo + r] << 8 | r;  // (subset, rank)
+        gsv[p] = sv;
       }
       nact += __popc(ok);
     }
     __syncwarp();
-    if (nact > 0) {
-      const int npairs = (int)(c.ee - c.eb) * nact;
-      // pair p0 + lane = (edge / nact, set % nact), advanced incrementally by
-      // 32.  The relaxation loop makes no calls (a call's register
+    const int npairs = (int)(c.ee - c.eb) * nact;
+    int npmax = npairs;  // the warp runs until its largest chunk is done
+    for (int o = GROW_LANES; o < 32; o <<= 1) npmax = max(npmax, __shfl_xor_sync(0xffffffffu, npmax, o));
+    if (npmax > 0) {
+      // pair p0 + sl = (edge / nact, set % nact), advanced incrementally by
+      // GROW_LANES.  The relaxation loop makes no calls (a call's register
       // convention would cost it occupancy): candidates that beat their
       // target are queued in shared memory and handled between batches.
-      const int q32 = 32 / nact, r32 = 32 % nact;
-      int e = (int)c.eb + lane / nact, bi = lane % nact;
+      const int na = nact > 0 ? nact : 1;
+      const int qG = GROW_LANES / na, rG = GROW_LANES % na;
+      int e = (int)c.eb + sl / na, bi = sl % na;
       int p0 = 0;
       while (true) {
         int nb = 0;  // queued candidates (warp-uniform)
-        for (; p0 < npairs && nb <= GROW_QUEUE - 32; p0 += 32) {
+        for (; p0 < npmax && nb <= GROW_QUEUE - 32; p0 += GROW_LANES) {
           int nc = INF, rS = 0;
           int2 a = make_int2(0, 0);
-          if (p0 + lane < npairs) {
+          if (p0 + sl < npairs) {
             a = __ldg(&g.adj[e]);
-            rS = s_r[wib][bi];
-            nc = s_sv[wib][bi] + a.y;
+            rS = gr[bi];
+            nc = gsv[bi] + a.y;
             ++nrel;
             if (use_dead && ((q.dead[(uint32_t)a.x >> 5] >> (a.x & 31)) & 1u)) nc = INF;
           }
-          e += q32;
-          bi += r32;
-          if (bi >= nact) { bi -= nact; ++e; }
+          e += qG;
+          bi += rG;
+          if (bi >= na) { bi -= na; ++e; }
           bool imp = false;
           if (nc < INF) {
             const int32_t* trow = q.table + (long long)a.x * rowlen;
@@ -1044,7 +1062,7 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
         for (int x = lane; x < nb; x += 32)
           nimp += grow_improve(q, g.V, (uint32_t)s_qu[wib][x], s_qr[wib][x], s_qc[wib][x], td, dist);
         __syncwarp();
-        if (p0 >= npairs) break;
+        if (p0 >= npmax) break;
       }
     }
     __syncwarp();
