@@ -588,21 +588,32 @@ __device__ __forceinline__ bool merge_item(Slot& q, int t, uint32_t v, int r, in
     // is at least max_{i in S} dist_i(v): skip the split loop when even that
     // cannot pass the lower-bound test
     int need = 0;
+    bool miss = false;  // a group of S has no entry at v
     for (int i = 0; i < k; ++i) {
       int dm = INF;
       for (int l = 0; l < L; ++l) dm = imin(dm, row[(1 + i) * L + l]);
       dist[i] = clip_dist(dm, q.R1);
-      if ((S >> i) & 1) need = imax(need, dist[i]);
+      if ((S >> i) & 1) {
+        need = imax(need, dist[i]);
+        miss |= dm >= INF;
+      }
     }
+    // R1 >= INF / 2: layer 1 ran untruncated (best was still unknown), so a
+    // missing singleton entry means the group is out of reach (for a
+    // D-query: more than D hops away) and every state (v, S) is infinite
+    if (miss && q.R1 >= INF / 2) return false;
     lbv = lower_bound(dist, k, W, S, q.lbtab);
     if ((long long)need + lbv > best) return false;
   } else {
     // full join: the answer at v is a tree rooted at v touching every group
+    bool miss = false;
     for (int i = 0; i < k; ++i) {
       int dm = INF;
       for (int l = 0; l < L; ++l) dm = imin(dm, row[(1 + i) * L + l]);
       dist[i] = clip_dist(dm, q.R1);
+      miss |= dm >= INF;
     }
+    if (miss && q.R1 >= INF / 2) return false;
     if (full_bound(dist, k, W, q.lbtab) > best) return false;
   }
   int M[LT > 0 ? LT : MAXL];
