@@ -448,6 +448,9 @@ def main():
     value = world * nq * args.steps / tot_dev
     e2e = world * nq * args.steps / tot_wall
     single_qps = nsingle / (single_ms / 1e3) if single_ms > 0 else None
+    # the one-per-call sample is the first nsingle queries: comparable with the
+    # batch only when every query has the same shape (same k, same kind)
+    uniform = len({(len(q), D >= 0) for q, D in zip(queries, Ds)}) == 1
 
     peak, peak_kind = peaks()
     grow_reads = sums["relax"] / (grow_ms / 1e3) if grow_ms > 0 else None
@@ -473,7 +476,8 @@ def main():
                 "d2h_bytes_per_step": d2h // args.steps},
         "gpu_launches": launches,
         "single_query_qps": single_qps,
-        "batched_over_single": (value / world) / single_qps if single_qps else None,
+        "single_query_sample": f"first {nsingle} queries, one per call" if nsingle else None,
+        "batched_over_single": (value / world) / single_qps if single_qps and uniform else None,
         "latency_ms_in_batch": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
                                 "p99": float(np.percentile(lat, 99))},
         "state_relaxations_per_s": world * sums["relax"] / tot_dev,
