@@ -154,7 +154,7 @@ class Engine {
     profile_ = c.profile != 0;
     bucket_shift_ = c.bucket_shift > 0 ? std::min(c.bucket_shift, 30) : 30;
     rounds_per_poll_ = c.rounds_per_poll > 0 ? c.rounds_per_poll : 8;
-    if (const char* w = std::getenv("GST_WATCHDOG_S")) watchdog_s_ = std::max(1.0, std::atof(w));
+    if (const char* w = std::getenv("GST_WATCHDOG_S")) watchdog_s_ = std::max(1e-4, std::atof(w));
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
       return fail(GST_E_CUDA, "no CUDA device visible");
@@ -533,7 +533,7 @@ class Engine {
       if (q != cudaErrorNotReady) return fail(GST_E_CUDA, std::string("engine stream: ") + cudaGetErrorString(q));
       if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > watchdog_s_) {
         broken_ = true;
-        return fail(GST_E_CUDA, "engine stream did not finish within " + std::to_string((int)watchdog_s_) +
+        return fail(GST_E_CUDA, "engine stream did not finish within " + std::to_string(watchdog_s_) +
                                     " s (GST_WATCHDOG_S); the engine is unusable");
       }
       if (spin > 2000) std::this_thread::sleep_for(std::chrono::microseconds(100));
