@@ -111,7 +111,11 @@ __device__ __forceinline__ int clip_dist(int d, int R1) { return d > R1 ? R1 + 1
 // layer (same |S|) runs the same (k - |S|)^2 iterations.  ceil(t / 2) is
 // monotone in t, so the tour bound rounds its minimum once.
 __device__ __forceinline__ int lower_bound(const int* dist, int k, int W, int S,
-                                           const int32_t* lbtab) {
+                                           const int32_t* lbtab, long long lim) {
+  // Callers only ask whether the bound exceeds lim, so the parts are taken
+  // cheapest first (one-label O(m), W2 tour O(m), pairwise tour O(m^2), m =
+  // |X|) and the first that exceeds lim ends the evaluation; a bound <= lim
+  // is the exact maximum of the three.
   const int Xs = (W - 1) ^ S;
   if (Xs == 0) return 0;
   int one = 0, mind = INF;
@@ -120,8 +124,16 @@ __device__ __forceinline__ int lower_bound(const int* dist, int k, int W, int S,
     one = imax(one, d);
     mind = imin(mind, d);
   }
-  long long t1 = 2LL * INF, lb2 = 0;
+  long long lb = one;
+  if (lb > lim) return (int)(lb < INF ? lb : INF);
   const int32_t* W2 = lbtab + (size_t)k * k * W + Xs;
+  for (int x = Xs; x; x &= x - 1) {
+    const int i = __ffs(x) - 1;
+    const long long t2 = ((long long)dist[i] + W2[i * W] + mind + 1) >> 1;
+    if (t2 > lb) lb = t2;
+  }
+  if (lb > lim) return (int)(lb < INF ? lb : INF);
+  long long t1 = 2LL * INF;
   for (int x = Xs; x; x &= x - 1) {
     const int i = __ffs(x) - 1;
     const long long di = dist[i];
@@ -131,13 +143,9 @@ __device__ __forceinline__ int lower_bound(const int* dist, int k, int W, int S,
       const long long t = di + Pi[j * W] + dist[j];
       if (t < t1) t1 = t;
     }
-    const long long t2 = (di + W2[i * W] + mind + 1) >> 1;
-    if (t2 > lb2) lb2 = t2;
   }
   const long long lb1 = (t1 + 1) >> 1;
-  long long lb = one;
   if (lb1 > lb && lb1 < INF) lb = lb1;
-  if (lb2 > lb) lb = lb2;
   return (int)(lb < INF ? lb : INF);
 }
 
@@ -602,7 +610,7 @@ __device__ __forceinline__ bool merge_item(Slot& q, int t, uint32_t v, int r, in
     // missing singleton entry means the group is out of reach (for a
     // D-query: more than D hops away) and every state (v, S) is infinite
     if (miss && q.R1 >= INF / 2) return false;
-    lbv = lower_bound(dist, k, W, S, q.lbtab);
+    lbv = lower_bound(dist, k, W, S, q.lbtab, (long long)best - need);
     if ((long long)need + lbv > best) return false;
   } else {
     // full join: the answer at v is a tree rooted at v touching every group
@@ -891,7 +899,7 @@ __device__ __forceinline__ bool lb_prunes(const int32_t* trow, int k, int W, int
     for (int l = 0; l < L; ++l) dm = imin(dm, trow[(1 + i) * L + l]);
     dist[i] = clip_dist(dm, R1);
   }
-  return (long long)nc + lower_bound(dist, k, W, S, lbtab) > best;
+  return (long long)nc + lower_bound(dist, k, W, S, lbtab, (long long)best - nc) > best;
 }
 
 // Adds a warp's relaxation counters to its slot (one atomic pair per flush).
