@@ -547,9 +547,12 @@ __device__ __forceinline__ void merge_costs(const int32_t* row, const uint8_t* s
       M[l] = m;
     }
   }
-  for (int S1 = (S - 1) & S; S1 > 0; S1 = (S1 - 1) & S) {
-    const int S2 = S ^ S1;
-    if (S1 < S2) continue;
+  // each unordered split once: S1 holds the highest group of S, S2 = S ^ S1
+  // is a non-empty part of the rest (2^(s-1) - 1 iterations, none wasted)
+  const int top = 1 << (31 - __clz(S));
+  const int rest = S ^ top;
+  for (int T = (rest - 1) & rest; rest != 0; T = (T - 1) & rest) {
+    const int S1 = top | T, S2 = rest ^ T;
     const int i1 = sidx[S1] * L, i2 = sidx[S2] * L;
     if (LT == 1) {
       M[0] = imin(M[0], row[i1] + row[i2]);
@@ -571,6 +574,7 @@ __device__ __forceinline__ void merge_costs(const int32_t* row, const uint8_t* s
         M[l] = imin(M[l], imin(a[l] + b[m2], a[m2] + b[l]));
       }
     }
+    if (T == 0) break;
   }
 #pragma unroll
   for (int l = 1; l < (LT > 0 ? LT : MAXL); ++l) {
