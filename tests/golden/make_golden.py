@@ -7,7 +7,7 @@ PrunedDP++ and D-PrunedDP++ binaries (oracle/_ref/).  The fixtures store the
 generator parameters, a checksum of the generated arrays (so a test can tell
 that it regenerated the same inputs) and the costs the reference printed.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [name ...]
 """
 from __future__ import annotations
 
@@ -50,6 +50,11 @@ DATASETS = {
                groups=dict(G=500, seed=101, uniform=[2, 20]),
                queries=[dict(k=3, n=50, seed=201)],
                hop=[dict(k=3, D=3, n=20)]),
+    # the C2 benchmark graph and groups (170k vertices, 3,000 groups): parity at full size
+    "c2": dict(graph=dict(V=170000, m=20, wmin=1, wmax=100, seed=1, path=True),
+               groups=dict(G=3000, seed=101, geometric=[8, 2, 200]),
+               queries=[dict(k=5, n=12, seed=201)],
+               hop=[dict(k=5, D=4, n=3), dict(k=5, D=5, n=3)]),
 }
 
 
@@ -118,8 +123,10 @@ def run_ref(g, gr, queries, hop_specs, name):
     return out
 
 
-def main():
+def main(names=None):
     for name, spec in DATASETS.items():
+        if names and name not in names:
+            continue
         g, gr, queries = build(spec)
         res = run_ref(g, gr, queries, spec["hop"], name)
         fx = dict(name=name, spec=spec, checksum=checksum(g, gr),
@@ -129,6 +136,8 @@ def main():
         with open(os.path.join(HERE, f"{name}.json"), "w") as f:
             json.dump(fx, f, indent=1)
         print(name, "done")
+    if names and "edge" not in names:
+        return
     g, gr, queries = edge_case_dataset()
     res = run_ref(g, gr, queries, [dict(k=3, D=2, n=6)], "edge")
     fx = dict(name="edge", checksum=checksum(g, gr),
@@ -142,4 +151,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])  # dataset names to (re)generate; none: all

@@ -85,3 +85,24 @@ def test_c3_shaped_k7_diameter_bound():
     for q, D, r in zip(qs, [3, 4, 5], batch):
         assert r.cost == e.solve(q, D).cost
     e.close()
+
+
+def test_c2_equals_the_reference_binaries(golden):
+    """The C2 benchmark graph and groups, 12 plain queries and 6 D-queries
+    (D = 4, 5): costs equal what the reference PrunedDP++ / D-PrunedDP++
+    printed (tests/golden/c2.json), batched and one per call."""
+    fx, g, gr = golden("c2")
+    e = gst_b200.Engine(device=0, arena_bytes=8 << 30, max_rounds=500000)
+    e.load_graph(g.rowptr, g.col, g.w)
+    e.load_groups(gr.ptr, gr.mem)
+    qs = fx["queries"]["5"]
+    got = [r.cost for r in e.solve_batch(qs)]
+    assert got == fx["reference"]["prunedpp"]["5"]
+    assert e.solve(qs[0]).cost == got[0]
+    for h in fx["reference"]["hop"]:
+        batch = e.solve_batch(qs[: h["n"]], [h["D"]] * h["n"])
+        assert [r.cost for r in batch] == h["costs"], h["D"]
+        for q, r in zip(qs, batch):
+            if r.feasible:
+                assert oracle.validate(g, gr, q, r.edges, r.root, r.cost, h["D"]) == 0
+    e.close()

@@ -69,3 +69,13 @@ def test_validator_rejects_bad_trees(golden):
     bad = edges.copy()
     bad[0, 2] += 1
     assert oracle.validate(g, gr, ids, bad, root, cost) == 1              # weight mismatch
+
+
+def test_c2_fixture_regenerates_and_pins_the_restatement(golden):
+    """The full-size C2 fixture: the generator reproduces the benchmark graph
+    (checksum), and the restatement equals the reference on its first two
+    plain queries (a few seconds each; the GPU test covers all of them)."""
+    fx, g, gr = golden("c2")
+    qs, want = fx["queries"]["5"], fx["reference"]["prunedpp"]["5"]
+    for ids, w in zip(qs[:2], want[:2]):
+        assert oracle.prunedpp(g, gr, ids)[0] == w
