@@ -21,7 +21,12 @@
 //     PrunedDP++ Theorem 1, CPUNONHOP.h:795);
 //   * a state is dropped when cost + lb(v, S) > best, lb the max of the
 //     one-label bound and the two tour bounds of LB_procedure (rounded up:
-//     the tree cost is an integer at least half the tour).
+//     the tree cost is an integer at least half the tour);
+//   * a vertex whose whole-tree lower bound exceeds best is dropped from the
+//     later merges (live lists) and, for the plain problem, from grows and
+//     preps (dead bitmap): no tree of cost <= best passes through it;
+//   * after an untruncated layer 1, a missing singleton entry means the group
+//     is out of reach, so every (v, S) containing it is skipped.
 // All kernels run on a fixed grid and read their work sizes from device
 // memory, so a round (ctl_a, lbprep, merge, prep, ctl_b, grow) can be captured
 // once in a CUDA graph and replayed.
@@ -45,7 +50,6 @@ constexpr int GROW_QUEUE = 128;  // improving candidates queued per warp
 // the per-chunk latency (descriptor, source row, dirty sets) overlaps.
 constexpr int GROW_LANES = 16;
 constexpr int GROW_CPW = 32 / GROW_LANES;  // chunks per warp
-
 
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
