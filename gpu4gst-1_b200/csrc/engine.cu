@@ -120,27 +120,6 @@ struct Request {
   cudaEvent_t t0 = nullptr;
 };
 
-static void fill_subset_tables(SubsetTables& t) {
-  std::memset(&t, 0, sizeof t);
-  for (int k = 1; k <= MAXK; ++k) {
-    const int W = 1 << k;
-    std::vector<int> order(W);
-    for (int S = 0; S < W; ++S) order[S] = S;
-    std::stable_sort(order.begin(), order.end(),
-                     [](int a, int b) { return __builtin_popcount(a) < __builtin_popcount(b); });
-    for (int i = 0; i < W; ++i) {
-      t.sof[k][i] = (uint8_t)order[i];
-      t.sidx[k][order[i]] = (uint8_t)i;
-    }
-    for (int s = 0; s <= k + 1; ++s) {
-      int c = 0;
-      for (int S = 0; S < W; ++S)
-        if (__builtin_popcount(S) < s) ++c;
-      t.loff[k][s] = (uint8_t)(s <= k ? c : W);
-    }
-  }
-}
-
 class Engine {
  public:
   ~Engine() { shutdown(); }

@@ -133,6 +133,31 @@ struct SubsetTables {
   uint8_t loff[MAXK + 1][MAXK + 2]; // first index of layer s
 };
 
+// Fills the subset orderings: for each k, the 2^k subsets ordered by
+// popcount and then by value; loff[k][s] is the index of the first set of
+// popcount s (loff[k][k + 1] = 2^k).  Host code; the engine and the
+// allocation-free entry point upload the same tables.
+inline void fill_subset_tables(SubsetTables& t) {
+  for (int k = 0; k <= MAXK; ++k)
+    for (int i = 0; i < MAXW; ++i) t.sidx[k][i] = t.sof[k][i] = 0;
+  for (int k = 0; k <= MAXK; ++k)
+    for (int s = 0; s < MAXK + 2; ++s) t.loff[k][s] = 0;
+  for (int k = 1; k <= MAXK; ++k) {
+    const int W = 1 << k;
+    int pos = 0;
+    for (int s = 0; s <= k; ++s) {
+      t.loff[k][s] = (uint8_t)pos;
+      for (int S = 0; S < W; ++S)
+        if (__builtin_popcount(S) == s) {
+          t.sof[k][pos] = (uint8_t)S;
+          t.sidx[k][S] = (uint8_t)pos;
+          ++pos;
+        }
+    }
+    t.loff[k][k + 1] = (uint8_t)W;
+  }
+}
+
 struct Graph {
   const long long* rowptr;  // V+1
   const int2* adj;          // E x (neighbour, weight)

@@ -1051,7 +1051,9 @@ k_grow(Slot* slots, const Plan* plan, Graph g) {
       // target are queued in shared memory and handled between batches.
       const int na = nact > 0 ? nact : 1;
       const int qG = GROW_LANES / na, rG = GROW_LANES % na;
-      int e = (int)c.eb + sl / na, bi = sl % na;
+      // unsigned: CSR offsets go up to 2^32 - 1 (the loaders' limit)
+      uint32_t e = c.eb + (uint32_t)(sl / na);
+      int bi = sl % na;
       int p0 = 0;
       while (true) {
         int nb = 0;  // queued candidates (warp-uniform)

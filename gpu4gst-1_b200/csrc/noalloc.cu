@@ -18,12 +18,22 @@
 // different streams of one device) race on it and must be serialised by the
 // caller.  The first call on a device does a one-time set-up on that device
 // (symbol address lookup, subset tables); make that first
-// call before any stream capture.
+// call before any stream capture.  Every call checks a token that the set-up
+// wrote into this library's device memory: a context that was reset and
+// re-created has lost it, so the set-up runs again there.
+//
+// Device waits are bounded like the engine's: a wait that does not end within
+// GST_WATCHDOG_S seconds (environment variable, default 120) fails the call
+// with GST_E_CUDA, and later calls on that device are refused, since the
+// scratch array may still be in use by the unfinished work.
 #include <cuda_runtime.h>
 
+#include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 
 #include "status.hpp"  // gst::fail: the library's shared error text
 
@@ -43,49 +53,87 @@ constexpr size_t kScratchBytes = GST_NOALLOC_SCRATCH_BYTES;
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
+// Written by the set-up; a module loaded into a fresh context starts at 0.
+constexpr unsigned kSetupToken = 0x6e6f616cu;
+static __device__ unsigned g_setup_token;
 
 struct DeviceSetup {
   bool done = false;
+  bool broken = false;            // a device wait ran out: refuse further calls
   unsigned char* base = nullptr;  // device address of g_scratch
 };
 DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mu;
 
-void fill_tables(SubsetTables& t) {
-  std::memset(&t, 0, sizeof t);
-  for (int k = 1; k <= MAXK; ++k) {
-    const int W = 1 << k;
-    int pos = 0;
-    for (int s = 0; s <= k; ++s) {
-      t.loff[k][s] = (uint8_t)pos;
-      for (int S = 0; S < W; ++S)
-        if (__builtin_popcount(S) == s) {
-          t.sof[k][pos] = (uint8_t)S;
-          t.sidx[k][S] = (uint8_t)pos;
-          ++pos;
-        }
+// Symbol address of the scratch array, subset tables and the set-up token,
+// with the device current.
+gst_status setup_device(int dev, DeviceSetup& s) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+  if (e != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  SubsetTables t;
+  fill_subset_tables(t);
+  e = cudaMemcpyToSymbol(c_sub, &t, sizeof t);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_setup_token, &kSetupToken, sizeof kSetupToken);
+  if (e != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: set-up: ") + cudaGetErrorString(e));
+  s.base = static_cast<unsigned char*>(p);
+  s.done = true;
+  (void)dev;
+  return GST_OK;
+}
+
+double watchdog_seconds() {
+  const char* w = std::getenv("GST_WATCHDOG_S");
+  const double x = w ? std::atof(w) : 120.0;
+  return x > 1e-4 ? x : 1e-4;
+}
+
+// Waits for the stream with a deadline (no event: nothing is created).
+gst_status wait_stream(cudaStream_t st, DeviceSetup& ds) {
+  const double limit = watchdog_seconds();
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int spin = 0;; ++spin) {
+    const cudaError_t q = cudaStreamQuery(st);
+    if (q == cudaSuccess) return GST_OK;
+    if (q != cudaErrorNotReady) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(q));
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > limit) {
+      ds.broken = true;
+      return fail(GST_E_CUDA, "noalloc: device work did not finish within " + std::to_string(limit) +
+                                  " s (GST_WATCHDOG_S); further calls on this device are refused");
     }
-    t.loff[k][k + 1] = (uint8_t)W;
+    if (spin > 2000) std::this_thread::sleep_for(std::chrono::microseconds(100));
+    else std::this_thread::yield();
   }
 }
 
-gst_status setup_device(int dev, unsigned char** base) {
-  std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (dev < 0 || dev >= kMaxDevices) return fail(GST_E_INVALID, "noalloc: device ordinal out of range");
-  DeviceSetup& s = g_setup[dev];
-  if (!s.done) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    SubsetTables t;
-    fill_tables(t);
-    e = cudaMemcpyToSymbol(c_sub, &t, sizeof t);
-    if (e != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: subset tables: ") + cudaGetErrorString(e));
-    s.base = static_cast<unsigned char*>(p);
-    s.done = true;
+// Bucket width of the cost-ordered grows, as the engine computes it at graph
+// load: the mean over vertices with edges of their lightest edge weight,
+// rounded, at least 1.  acc[0] = sum, acc[1] = count (cleared by the caller).
+__global__ void k_delta_sum(Graph g, unsigned long long* acc) {
+  unsigned long long sum = 0, cnt = 0;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < g.V;
+       v += (long long)gridDim.x * blockDim.x) {
+    const long long b = g.rowptr[v], e = g.rowptr[v + 1];
+    if (e == b) continue;
+    int mn = INT32_MAX;
+    for (long long j = b; j < e; ++j) mn = imin(mn, g.adj[j].y);
+    sum += (unsigned long long)mn;
+    ++cnt;
   }
-  *base = s.base;
-  return GST_OK;
+  for (int o = 16; o; o >>= 1) {
+    sum += __shfl_down_sync(0xffffffffu, sum, o);
+    cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+  }
+  if ((threadIdx.x & 31) == 0 && cnt) {
+    atomicAdd(&acc[0], sum);
+    atomicAdd(&acc[1], cnt);
+  }
+}
+
+__global__ void k_delta_set(Slot* q, const unsigned long long* acc) {
+  const double m = acc[1] ? (double)acc[0] / (double)acc[1] : 1.0;
+  const int d = (int)(m + 0.5);
+  q->delta = d > 1 ? d : 1;
 }
 
 size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -98,7 +146,8 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
                                         const int32_t* d_group_members, const int32_t* group_ids, int k,
                                         int D, void* stream, int64_t* cost_out, int32_t* root_out) {
   using namespace gst_noalloc;
-  if (!d_rowptr || !d_adj || !d_group_ptr || !group_ids || !cost_out || !root_out || V <= 0 || E < 0 || k <= 0)
+  if (!d_rowptr || !d_adj || !d_group_ptr || !d_group_members || !group_ids || !cost_out || !root_out ||
+      V <= 0 || E < 0 || k <= 0)
     return fail(GST_E_INVALID, "noalloc: null pointer or empty input");
   if (V > INT32_MAX || E >= (int64_t)UINT32_MAX) return fail(GST_E_UNSUPPORTED, "noalloc: graph too large");
   if (D > GST_MAX_D) return fail(GST_E_UNSUPPORTED, "noalloc: D above GST_MAX_D");
@@ -118,27 +167,37 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   int dev = 0;
   cudaError_t ce = cudaGetDevice(&dev);
   if (ce != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(ce));
-  unsigned char* base = nullptr;
-  gst_status st = setup_device(dev, &base);
-  if (st != GST_OK) return st;
+  if (dev < 0 || dev >= kMaxDevices) return fail(GST_E_INVALID, "noalloc: device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_setup_mu);  // one call per process at a time: they share the array
+  DeviceSetup& ds = g_setup[dev];
+  if (ds.broken) return fail(GST_E_STATE, "noalloc: an earlier call on this device timed out");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-
-  // group sizes (host copies of two offsets per queried group)
-  for (int i = 0; i < kk; ++i) {
-    int64_t b[2];
-    ce = cudaMemcpyAsync(b, d_group_ptr + groups[i], sizeof b, cudaMemcpyDeviceToHost, s);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-    if (ce != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(ce));
-    if (b[1] == b[0]) return GST_OK;  // an empty group: infeasible
+  if (!ds.done) {
+    gst_status st = setup_device(dev, ds);
+    if (st != GST_OK) return st;
   }
+  unsigned char* base = ds.base;
+
+  // group offsets (two per queried group) and the set-up token, in one wait
+  int64_t goff[MAXK][2];
+  unsigned token = 0;
+  for (int i = 0; i < kk && ce == cudaSuccess; ++i)
+    ce = cudaMemcpyAsync(goff[i], d_group_ptr + groups[i], sizeof goff[i], cudaMemcpyDeviceToHost, s);
+  if (ce == cudaSuccess) ce = cudaMemcpyFromSymbolAsync(&token, g_setup_token, sizeof token, 0, cudaMemcpyDeviceToHost, s);
+  if (ce != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(ce));
+  if (gst_status st = wait_stream(s, ds); st != GST_OK) return st;
+  if (token != kSetupToken) {  // the context was reset since the set-up
+    gst_status st = setup_device(dev, ds);
+    if (st != GST_OK) return st;
+    base = ds.base;
+  }
+  for (int i = 0; i < kk; ++i)
+    if (goff[i][1] == goff[i][0]) return GST_OK;  // an empty group: infeasible
   if (kk == 1) {  // one group: any member is a tree of cost 0
     int32_t m = 0;
-    int64_t b = 0;
-    ce = cudaMemcpyAsync(&b, d_group_ptr + groups[0], sizeof b, cudaMemcpyDeviceToHost, s);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&m, d_group_members + b, sizeof m, cudaMemcpyDeviceToHost, s);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    ce = cudaMemcpyAsync(&m, d_group_members + goff[0][0], sizeof m, cudaMemcpyDeviceToHost, s);
     if (ce != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(ce));
+    if (gst_status st = wait_stream(s, ds); st != GST_OK) return st;
     *cost_out = 0;
     *root_out = m;
     return GST_OK;
@@ -162,6 +221,7 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   const size_t o_chunks = take(chunk_cap * sizeof(Chunk));
   const size_t o_lbtab = take((size_t)kk * kk * W * 4 + (size_t)kk * W * 4);
   const size_t o_live = take(2 * (size_t)V * 4);
+  const size_t o_acc = take(2 * sizeof(unsigned long long));
   if (off > kScratchBytes)
     return fail(GST_E_NOMEM, "noalloc: query needs " + std::to_string(off >> 20) + " MiB of scratch, above the " +
                                  std::to_string(kScratchBytes >> 20) + " MiB static maximum");
@@ -197,7 +257,7 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   q.best = INF;
   q.R1 = INF / 2;
   q.answer = ~0ull;
-  q.delta = 1;  // narrow first buckets: correct for any weights without a pass over the graph
+  q.delta = 1;  // replaced on the device by k_delta_set before the first round
   q.bshift = 30;
   q.T = 0;
   q.next_min = INF;
@@ -209,9 +269,10 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_tflag, 0, (size_t)V * 4, s);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_dead, 0, ((size_t)V + 31) / 32 * 4, s);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(d_plan, 0, sizeof(Plan), s);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_acc, 0, 2 * sizeof(unsigned long long), s);
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_slot, &q, sizeof q, cudaMemcpyHostToDevice, s);
-  if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);  // q lives on this stack frame
   if (ce != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(ce));
+  if (gst_status st = wait_stream(s, ds); st != GST_OK) return st;  // q lives on this stack frame
 
   Graph g;
   g.rowptr = reinterpret_cast<const long long*>(d_rowptr);
@@ -224,6 +285,9 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int grid = nsm * 4;
+  unsigned long long* d_acc = reinterpret_cast<unsigned long long*>(base + o_acc);
+  k_delta_sum<<<grid, 256, 0, s>>>(g, d_acc);
+  k_delta_set<<<1, 1, 0, s>>>(d_slot, d_acc);
   k_init_seeds<<<64, 256, 0, s>>>(d_slot, 0, g);
   k_init_base<<<64, 256, 0, s>>>(d_slot, 0, g);
   const long long max_rounds = 4ll * V * (long long)L + 1000;  // far above any DP's need
@@ -242,8 +306,8 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
     k_publish<<<1, 32, 0, s>>>(d_slot, 1, d_status);
     ce = cudaGetLastError();
     if (ce == cudaSuccess) ce = cudaMemcpyAsync(&hs, d_status, sizeof hs, cudaMemcpyDeviceToHost, s);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
     if (ce != cudaSuccess) return fail(GST_E_CUDA, std::string("noalloc: ") + cudaGetErrorString(ce));
+    if (gst_status st = wait_stream(s, ds); st != GST_OK) return st;
     if (hs.phase == PH_DONE || hs.phase == PH_ERROR) break;
     if (rounds > max_rounds) return fail(GST_E_LIMIT, "noalloc: round limit exceeded");
   }

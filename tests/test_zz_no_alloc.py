@@ -55,6 +55,7 @@ def test_noalloc_equals_solve_on_two_calls_in_a_row(golden, name):
     for k, qs in fx["queries"].items():
         for ids in qs[:3]:
             cases += [(ids, -1), (ids, 3)]
+        cases.append((qs[0], 0))  # D = 0: one label, its own sizing path
     for ids, D in cases:
         want = e.solve(ids, D)
         for _ in range(2):
@@ -75,3 +76,35 @@ def test_noalloc_rejects_queries_beyond_its_scratch(golden):
     st, cost, root = _noalloc(lib, g, gr, dev, list(range(7)), 15)
     assert st == 5  # GST_E_NOMEM
     assert b"static maximum" in lib.gst_last_error()
+
+
+def test_noalloc_wide_weights_and_no_device_allocation():
+    """Weights U[1,1000] on a 20,000-vertex graph (the bucket width comes from
+    the graph, as in the engine), compared with gst_solve; after a warm-up
+    call, further calls leave the device's free memory unchanged: the entry
+    point allocates nothing, and nothing it loads grows later."""
+    import torch
+    from gst_b200 import datagen as dg
+    g = dg.ba_graph(20000, 4, 1, 1000, seed=31, spanning_path=True)
+    gr = dg.make_groups(g.V, 300, seed=32, geometric=(8, 2, 100))
+    qs = [q for q, _ in dg.make_queries(gr.n, 6, [3, 4, 5], seed=33)]
+    lib = gst_b200.load_library()
+    dev = _device_inputs(torch, g, gr)
+    torch.cuda.synchronize()
+    e = gst_b200.Engine(device=0, arena_bytes=1 << 30, max_rounds=200000)
+    e.load_graph(g.rowptr, g.col, g.w)
+    e.load_groups(gr.ptr, gr.mem)
+    cases = [(q, D) for q in qs for D in (-1, 2)]
+    want = [e.solve(q, D) for q, D in cases]
+    e.close()
+    torch.cuda.synchronize()
+    st, _, _ = _noalloc(lib, g, gr, dev, cases[0][0], cases[0][1])  # warm-up
+    assert st == 0, lib.gst_last_error()
+    free0, _ = torch.cuda.mem_get_info()
+    for (q, D), w in zip(cases, want):
+        st, cost, root = _noalloc(lib, g, gr, dev, q, D)
+        assert st == 0, lib.gst_last_error()
+        assert cost == w.cost, (list(q), D, cost, w.cost)
+        assert root == (w.root if w.feasible else -1)
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
