@@ -1,22 +1,32 @@
 """Benchmark: GST queries/s on one B200 (or N replicas), exact costs.
 
 A "step" is one batch of queries solved by the engine over the resident
-graph (default workload C2: BA V=170,000 m=20 + spanning path, w U[1,100],
-3,000 groups Geom(8) in [2,200], 300 queries of k=5; seeded synthetic data
-standing in for the reference's external social graphs).
+graph.  The default workload is C4, the configuration the headline metric is
+stated on: BA V=4,000,000 m=9 + spanning path, w U[1,100], 20,000 groups
+Geom(12) in [2,1000], 300 queries with k uniform in {3,5,7}, half of them
+diameter-bounded (D uniform in [2,5]).  Seeded synthetic data stands in for
+the reference's external social graphs.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c4|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c4|c2|c1]
                     [--impl ours|reference]
+    python bench.py --workload c5 [--rates 50,200,1000] [--serve-queries 10000]
 
 Prints one JSON line (rank 0).  `value` is device-timed (CUDA events on the
 engine's stream) whole-job queries/s with the graph resident in HBM; `e2e`
 is the same metric through the C ABI with host buffers (query ids in, costs
-and tree edges out) timed by the host clock around the call.  `roofline` is
-the grow kernel's algorithmic bytes per second (events captured around each
-grow launch) against the measured HBM copy bandwidth.  `cpu_baseline` runs
-the reference's own PrunedDP++ (built from source into oracle/_ref) on a
-bounded sample of the same workload, one process per core as the reference's
-scripts do.  --impl reference times that reference CPU path alone.
+and tree edges out) timed by the host clock around the call.
+`single_query_qps` times the same engine one query per call on a sample of
+every (k, plain / D-bounded) class and weights the classes as the batch
+does; `batched_over_single` is the ratio.  `parity` compares the batch's
+costs with the reference costs committed under tests/golden/ for this
+workload.  `roofline` is the grow kernel's algorithmic bytes per second
+(events captured around each grow launch) against the measured HBM copy
+bandwidth.  `cpu_baseline` times the reference's own PrunedDP++ (built from
+source into oracle/_ref) on a bounded sample of the workload's plain
+queries, per query from its own progress lines (graph load excluded), and
+scales it to the host cores.  --impl reference times that reference CPU
+path alone.  --workload c5 is the serving loop: Poisson arrivals on the C4
+graph, one JSON line per arrival rate.
 """
 from __future__ import annotations
 
@@ -61,6 +71,54 @@ def make_workload(name: str, rank: int):
     else:
         raise SystemExit(f"unknown workload {name}")
     return wl
+
+
+def c5_queries(n_groups: int, n: int):
+    """The serving mix on the C4 graph and groups: k in {3,5,7} with
+    probabilities {0.5,0.3,0.2}; D unbounded with probability 0.5, else
+    uniform in [2,5]; seed 7."""
+    from gst_b200 import datagen as dg
+    return dg.make_queries(n_groups, n, ([3, 5, 7], [0.5, 0.3, 0.2]), 7,
+                           D=lambda r: -1 if r.random() < 0.5 else int(r.integers(2, 6)))
+
+
+def query_class(q, D) -> str:
+    return f"k{len(q)}_" + ("plain" if D < 0 else "D")
+
+
+def arrays_checksum(g, gr) -> str:
+    """sha256 prefix of the generated graph and group arrays (the recipe the
+    committed fixtures under tests/golden/ carry)."""
+    import hashlib
+    import numpy as np
+    h = hashlib.sha256()
+    for a in (g.rowptr, g.col, g.w, gr.ptr, gr.mem):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()[:16]
+
+
+def fixture_parity(name: str, wl, costs) -> dict | None:
+    """Compares the batch's costs with the reference costs committed in
+    tests/golden/<name>.json (the queries there are this workload's own, by
+    index).  Raises if one differs."""
+    path = os.path.join(ROOT, "tests", "golden", f"{name}.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        fx = json.load(f)
+    if "cells" not in fx or fx.get("checksum") != arrays_checksum(wl.graph, wl.groups):
+        return None
+    n = 0
+    for c in fx["cells"]:
+        if not c.get("costs"):
+            continue
+        for i, want in zip(c["idx"], c["costs"]):
+            if want is None:
+                continue
+            assert costs[i] == want, f"query {i} (k={c['k']}, D={c['D']}): {costs[i]} != reference {want}"
+            n += 1
+    return {"fixture": f"tests/golden/{name}.json", "queries_checked": n, "equal": True,
+            "against": "reference PrunedDP++ / D-PrunedDP++ costs"}
 
 
 def filter_queries(wl, args):
@@ -176,51 +234,107 @@ def grow_bytes(stats_sum):
     return 16 * stats_sum["frontier"] + 12 * stats_sum["relax"] + 4 * stats_sum["improve"]
 
 
-def cpu_reference_sample(wl, name: str, n_queries: int, procs: int, timeout: float = 600):
-    """Runs the reference PrunedDP++ binary (oracle/_ref) on the first
-    n_queries queries of the workload, `procs` processes on disjoint query
-    ranges.  Returns (queries/s by wall clock, per-query reference CSV times, kind)."""
-    import oracle
+def write_dataset_files(name: str, out_dir: str) -> dict:
+    """Writes the workload's graph and groups in the reference's text formats
+    and its plain queries by k, from a child process, so that the process
+    timing the reference never maps this project's libraries.  Returns the
+    plain queries as {k: [[ids], ...]} in workload order."""
+    meta = os.path.join(out_dir, "meta.json")
+    if not os.path.exists(meta):
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--write-dataset", out_dir,
+                        "--workload", name], check=True, stdin=subprocess.DEVNULL)
+    with open(meta) as f:
+        return {int(k): v for k, v in json.load(f).items()}
+
+
+def _write_dataset_main(name: str, out_dir: str) -> None:
     from gst_b200 import datagen as dg
+    wl = make_workload(name, 0)
+    dg.write_dataset(out_dir, name, dg.Workload(wl.graph, wl.groups, []), binary=False)
+    byk = {}
+    for q, D in wl.queries:
+        if D < 0:
+            byk.setdefault(len(q), []).append([int(x) for x in q])
+    for k, qs in byk.items():
+        with open(os.path.join(out_dir, f"{name}{k}.csv"), "w") as f:
+            for q in qs:
+                f.write(" ".join(map(str, q)) + "\n")
+    with open(os.path.join(out_dir, "meta.json.tmp"), "w") as f:
+        json.dump(byk, f)
+    os.replace(os.path.join(out_dir, "meta.json.tmp"), os.path.join(out_dir, "meta.json"))
+
+
+def run_ref_timed(exe: str, d: str, name: str, k: int, a: int, b: int, budget_s: float):
+    """Runs the reference PrunedDP++ on queries a..b of <name><k>.csv and
+    times each query from its own progress lines ("<data> iteration i" is
+    printed when query i starts; the process ends after the last one), so
+    the graph load is excluded and each query's own preprocessing counted.
+    The process is stopped budget_s seconds after its first query started;
+    only the queries it finished are returned."""
+    p = subprocess.Popen([exe, "1", d + "/", name, str(k), str(a), str(b)], stdout=subprocess.PIPE,
+                         stderr=subprocess.DEVNULL, stdin=subprocess.DEVNULL, text=True)
+    starts = []
+    ended = []
+    timer = None
+
+    def stop():
+        if p.poll() is None:
+            p.kill()
+
+    for line in p.stdout:
+        if " iteration " in line:
+            starts.append(time.perf_counter())
+            if timer is None:
+                timer = threading.Timer(budget_s, stop)
+                timer.start()
+        elif "END" in line and "runningtime" in line:
+            ended.append(time.perf_counter())
+    p.wait()
+    if timer is not None:
+        timer.cancel()
+    bounds = starts[1:] + ended[:1]
+    return [t1 - t0 for t0, t1 in zip(starts, bounds)]
+
+
+def cpu_reference_sample(name: str, per_k: int, budget_s: float = 600):
+    """The reference PrunedDP++ (oracle/_ref) on the first per_k plain
+    queries of each k of the workload, one single-threaded process per query,
+    all at once.  Returns per-class mean seconds per query and what ran."""
+    import oracle
     exe = oracle.ref_binary("PrunedDP++")
-    d = tempfile.mkdtemp(prefix="gstbench_")
-    plain = [(q, D) for q, D in wl.queries if D < 0]
-    ks = sorted({len(q) for q, _ in plain})
-    k = ks[0]
-    qs = [(q, D) for q, D in plain if len(q) == k][:n_queries]
-    dg.write_dataset(d, name, dg.Workload(wl.graph, wl.groups, []), binary=False)
-    dg.write_queries(os.path.join(d, f"{name}{k}.csv"), qs)
-    per = max(1, (len(qs) + procs - 1) // procs)
-    ranges = [(s, min(s + per, len(qs)) - 1) for s in range(0, len(qs), per)]
-    if os.path.exists(exe):
-        kind = "reference"
-        t0 = time.time()
-        ps = [subprocess.Popen([exe, "1", d + "/", name, str(k), str(a), str(b)], stdout=subprocess.DEVNULL,
-                               stderr=subprocess.DEVNULL, stdin=subprocess.DEVNULL) for a, b in ranges]
-        for p in ps:
-            p.wait(timeout=timeout)
-        wall = time.time() - t0
-        times = []
-        try:
-            for a, b in ranges:
-                fn = os.path.join(d, "result", f"exp_CPU_nonHop_{name}_T{k}_{a}-{b}.csv")
-                with open(fn) as f:
-                    next(f)
-                    for line in f:
-                        if line.strip():
-                            times.append(float(line.split(",")[2]))
-        except OSError:
-            pass
-        return len(qs) / wall, times, kind, len(ranges), len(qs), k
-    # no reference build on this box: the oracle port, one process per range
-    import multiprocessing as mp
-    kind = "port"
-    ctx = mp.get_context("spawn")
-    t0 = time.time()
-    with ctx.Pool(len(ranges)) as pool:
-        pool.starmap(_port_range, [(wl, [q for q, _ in qs[a:b + 1]]) for a, b in ranges])
-    wall = time.time() - t0
-    return len(qs) / wall, [], kind, len(ranges), len(qs), k
+    if not os.path.exists(exe):
+        return None
+    d = os.path.join(tempfile.gettempdir(), f"gstbench_{name}")
+    os.makedirs(os.path.join(d, "result"), exist_ok=True)
+    byk = write_dataset_files(name, d)
+    jobs = [(k, i) for k in sorted(byk) for i in range(min(per_k, len(byk[k])))]
+    out = [None] * len(jobs)
+
+    def one(j):
+        k, i = jobs[j]
+        out[j] = run_ref_timed(exe, d, name, k, i, i, budget_s)
+
+    ths = [threading.Thread(target=one, args=(j,)) for j in range(len(jobs))]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    per = {}
+    for (k, i), ts in zip(jobs, out):
+        if ts:
+            per.setdefault(k, []).append(ts[0])
+    return {"per_k_s": {k: statistics.mean(v) for k, v in per.items()}, "queries": len(jobs),
+            "per_k": per_k}
+
+
+def cpu_mix_qps(per_k_s: dict, queries, cores: int):
+    """Queries/s of `cores` single-threaded reference processes on the
+    plain-query mix of the workload (each class weighted by its count)."""
+    plain = [len(q) for q, D in queries if D < 0 and len(q) in per_k_s]
+    if not plain:
+        return None
+    mean_s = sum(per_k_s[k] for k in plain) / len(plain)
+    return cores / mean_s
 
 
 def reference_gpu_sample(wl, name: str, n: int, timeout: float = 900):
@@ -257,80 +371,123 @@ def reference_gpu_sample(wl, name: str, n: int, timeout: float = 900):
 
 
 def run_serving(args):
-    """Poisson arrivals at --serve queries/s through the engine's serving loop
-    (continuous batching); reports per-query latency from submit to result and
-    the sustained throughput."""
+    """C5: the serving loop (continuous batching) on the C4 graph and groups
+    under Poisson arrivals, one JSON line per rate.  Latency runs from a
+    query's submission to its result being ready on the host (measured by
+    the engine); every served cost must equal the engine's batch answer for
+    the same query, and the C4 batch is checked against the reference costs
+    of the C4 fixture."""
     import numpy as np
     import gst_b200
-    wl = make_workload(args.workload, 0)
-    filter_queries(wl, args)
-    eng = gst_b200.Engine(device=0, arena_bytes=int(args.arena_gb * (1 << 30)))
+    wl = make_workload("c4", 0)
+    queries = c5_queries(wl.groups.n, args.serve_queries)
+    eng = gst_b200.Engine(device=0, arena_bytes=int(args.arena_gb * (1 << 30)),
+                          max_slots=args.max_slots, rounds_per_poll=args.rounds_per_poll)
     eng.load_graph(wl.graph.rowptr, wl.graph.col, wl.graph.w)
     eng.load_groups(wl.groups.ptr, wl.groups.mem)
-    alone = eng.solve_batch([q for q, _ in wl.queries], [D for _, D in wl.queries])
-    rng = np.random.default_rng(7)
-    gaps = rng.exponential(1.0 / args.serve, size=len(wl.queries))
-    lat = [None] * len(wl.queries)
-    got = [None] * len(wl.queries)
-    with eng.server() as srv:
-        def waiter(i, ticket, t_sub):  # one waiter per request: latency = submit -> result
-            r = srv.wait(ticket)
-            lat[i] = time.perf_counter() - t_sub
-            got[i] = r.cost
-
-        ths = []
-        t0 = time.perf_counter()
-        t_next = t0
-        for i, (q, D) in enumerate(wl.queries):
-            t_next += gaps[i]
-            while time.perf_counter() < t_next:
-                time.sleep(0.0002)
-            t_sub = time.perf_counter()
-            th = threading.Thread(target=waiter, args=(i, srv.submit(q, D), t_sub))
-            th.start()
-            ths.append(th)
-        for th in ths:
-            th.join()
-        span = time.perf_counter() - t0
+    c4_costs = [r.cost for r in eng.solve_batch([q for q, _ in wl.queries], [D for _, D in wl.queries])]
+    parity = fixture_parity("c4", wl, c4_costs)
+    t0 = time.perf_counter()
+    alone = [r.cost for r in eng.solve_batch([q for q, _ in queries], [D for _, D in queries])]
+    batch_s = time.perf_counter() - t0
+    mix = {}
+    for q, D in queries:
+        mix[query_class(q, D)] = mix.get(query_class(q, D), 0) + 1
+    for rate in args.rates:
+        gaps = np.random.default_rng(7).exponential(1.0 / rate, size=len(queries))
+        tickets = []
+        sampler = ClockSampler(0)
+        sampler.start()
+        with eng.server() as srv:
+            t0 = time.perf_counter()
+            t_next = t0
+            for i, (q, D) in enumerate(queries):
+                t_next += gaps[i]
+                while True:
+                    dt = t_next - time.perf_counter()
+                    if dt <= 0:
+                        break
+                    time.sleep(min(dt, 0.001))
+                tickets.append(srv.submit(q, D))
+            res = [srv.wait(t) for t in tickets]
+            span = time.perf_counter() - t0
+        clocks = sampler.stop()
+        lat = np.array([r.stats["latency_ms"] for r in res])
+        qwait = np.array([r.stats["queue_ms"] for r in res])
+        got = [r.cost for r in res]
+        bad = sum(1 for a, b in zip(got, alone) if a != b)
+        assert all(r.status == 0 for r in res), "a served query failed"
+        print(json.dumps({
+            "mode": "serving", "workload": "C5: the C4 graph and groups; Poisson arrivals, seed 7; "
+            "k in {3,5,7} w.p. {.5,.3,.2}; D=inf w.p. .5, else U[2,5]",
+            "arrival_rate_qps": rate, "queries": len(queries), "mix": mix, "served_qps": len(queries) / span,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
+                           "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "admission_wait_ms": {"p50": float(np.percentile(qwait, 50)), "p99": float(np.percentile(qwait, 99))},
+            "results_equal_batch": bad == 0, "results_differing": bad,
+            "batch_same_queries_qps": len(queries) / batch_s,
+            "parity_c4": parity, "clocks": clocks}), flush=True)
+        assert bad == 0, f"{bad} served costs differ from the batch answer"
     eng.close()
-    ms = np.array(lat) * 1e3
-    print(json.dumps({
-        "mode": "serving", "workload": WORKLOADS[args.workload], "arrival_rate_qps": args.serve,
-        "queries": len(wl.queries), "served_qps": len(wl.queries) / span,
-        "latency_ms": {"p50": float(np.percentile(ms, 50)), "p90": float(np.percentile(ms, 90)),
-                       "p99": float(np.percentile(ms, 99)), "max": float(ms.max())},
-        "results_equal_alone": got == [r.cost for r in alone]}), flush=True)
-
-
-def _port_range(wl, queries):
-    import oracle
-    for q in queries:
-        oracle.prunedpp(wl.graph, wl.groups, q)
 
 
 def run_reference_arm(args):
+    """The reference's own CPU path (PrunedDP++ from oracle/_ref) on the host
+    cores, on this workload's plain queries.  One single-threaded process per
+    core; process p runs queries of class k = ks[p % len(ks)] one after
+    another (warm-up queries first), timed from the reference's own progress
+    lines (graph load excluded) and stopped after a time budget.  value =
+    cores / the mean time per query of the plain-query mix (each class
+    weighted by its share of the workload's plain queries): the throughput of
+    the host cores kept busy on that mix."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    wl = make_workload(args.workload, 0)
+    import oracle
+    exe = oracle.ref_binary("PrunedDP++")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/PrunedDP++ is not built"}), flush=True)
+        return
     procs = max(1, min(os.cpu_count() or 1, 32))
-    vals = []
-    info = None
-    for step in range(args.warmup + args.steps):
-        qps, times, kind, nproc, nq, k = cpu_reference_sample(wl, args.workload, procs, procs)
-        if step >= args.warmup:
-            vals.append(qps)
-        info = (kind, nproc, nq, k)
-    kind, nproc, nq, k = info
-    v = statistics.mean(vals) if vals else None
-    sample = (f"{nq} queries (k={k}) of the {args.workload.upper()} workload per step, one "
-              f"single-threaded PrunedDP++ process per query range, {nproc} processes")
+    d = os.path.join(tempfile.gettempdir(), f"gstbench_{args.workload}")
+    os.makedirs(os.path.join(d, "result"), exist_ok=True)
+    byk = write_dataset_files(args.workload, d)
+    ks = sorted(byk)
+    per = args.warmup + args.steps
+    got = {}
+
+    def one(p):
+        k = ks[p % len(ks)]
+        n = len(byk[k])
+        a = ((p // len(ks)) * per) % n
+        b = min(n, a + per) - 1
+        got[p] = (k, run_ref_timed(exe, d, args.workload, k, a, b, budget_s=args.ref_budget))
+
+    ths = [threading.Thread(target=one, args=(p,)) for p in range(procs)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    per_k = {}
+    for k, ts in got.values():
+        timed = ts[args.warmup:] if len(ts) > args.warmup else ts
+        per_k.setdefault(k, []).extend(timed)
+    mean_k = {k: statistics.mean(v) for k, v in per_k.items() if v}
+    weights = {k: len(v) for k, v in byk.items() if k in mean_k}
+    t_mix = sum(weights[k] * mean_k[k] for k in weights) / sum(weights.values())
+    v = procs / t_mix
+    nq = sum(len(v) for v in per_k.values())
+    sample = (f"{nq} timed plain queries of the {args.workload.upper()} workload on {procs} single-threaded "
+              f"PrunedDP++ processes (k per process cycling over {ks}, {args.warmup} warm-up queries each, "
+              f"stopped {args.ref_budget:.0f} s after the first query); per-query time from the reference's "
+              f"progress lines (graph load excluded); mean s per query by k: "
+              + ", ".join(f"k={k}: {mean_k[k]:.2f}" for k in sorted(mean_k)))
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.workload]},
-        "cpu_baseline": {"value": v, "unit": "queries/s", "cores": nproc, "kind": kind, "sample": sample},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_mix,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "config": {"workload": WORKLOADS[args.workload]},
+        "cpu_baseline": {"value": v, "unit": "queries/s", "cores": procs, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -340,9 +497,11 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c4", choices=sorted(WORKLOADS) + ["c5"],
+                    help="c5: the serving loop on the C4 graph")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--single", type=int, default=30, help="queries timed one per call")
+    ap.add_argument("--single-per-class", type=int, default=3,
+                    help="queries of each (k, plain / D-bounded) class timed one per call")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=0, help="queries per step (0: the workload's count)")
     ap.add_argument("--arena-gb", type=float, default=0.0, help="device arena size (0: 85%% of free memory)")
@@ -354,11 +513,17 @@ def main():
                     help="keep only plain (D unbounded) or diameter-bounded queries")
     ap.add_argument("--ref-gpu", type=int, default=0,
                     help="also run the reference GPU TrimCDP on this many plain queries (comparator)")
-    ap.add_argument("--serve", type=float, default=0.0,
-                    help="serving mode: Poisson arrivals at this many queries/s (prints its own line)")
+    ap.add_argument("--rates", default="50,200,1000", help="c5: Poisson arrival rates, queries/s")
+    ap.add_argument("--serve-queries", type=int, default=10000, help="c5: queries per rate")
+    ap.add_argument("--ref-budget", type=float, default=150.0,
+                    help="reference arm: seconds each reference process runs after its first query")
+    ap.add_argument("--write-dataset", default="", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.write_dataset:
+        return _write_dataset_main(args.workload, args.write_dataset)
     args.warmup = max(args.warmup, 3)
-    if args.serve > 0:
+    args.rates = [float(x) for x in args.rates.split(",") if x]
+    if args.workload == "c5":
         return run_serving(args)
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -379,6 +544,7 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     wl = make_workload(args.workload, rank)
+    unfiltered = not (args.k or args.kind != "all" or args.queries)
     filter_queries(wl, args)
     queries = [q for q, _ in wl.queries]
     Ds = [D for _, D in wl.queries]
@@ -429,14 +595,25 @@ def main():
         costs = c
     barrier()
     clocks = sampler.stop()
+    parity = fixture_parity(args.workload, wl, costs) if unfiltered else None
 
-    # one-query-per-call form of the same engine (the "plain" GPU form)
-    nsingle = min(args.single, len(queries))
-    single_ms = 0.0
-    for i in range(nsingle):
-        r = eng.solve(queries[i], Ds[i])
-        assert r.cost == costs[i], "one-query form disagrees with the batch"
-        single_ms += eng.profile()["run_ms"]
+    # one-query-per-call form of the same engine (the "plain" GPU form): the
+    # first queries of every (k, kind) class, weighted as the batch mixes them
+    classes = {}
+    for i, (q, D) in enumerate(zip(queries, Ds)):
+        classes.setdefault(query_class(q, D), []).append(i)
+    single = {}
+    for cl, idx in sorted(classes.items()):
+        ms = []
+        for i in idx[: args.single_per_class]:
+            r = eng.solve(queries[i], Ds[i])
+            assert r.cost == costs[i], "one-query form disagrees with the batch"
+            ms.append(eng.profile()["run_ms"])
+        if ms:
+            single[cl] = {"queries_in_batch": len(idx), "timed": len(ms), "mean_ms": statistics.mean(ms)}
+    single_qps = None
+    if single and all(cl in single for cl in classes):
+        single_qps = len(queries) / (sum(v["queries_in_batch"] * v["mean_ms"] for v in single.values()) / 1e3)
 
     nq = len(queries)
     tot_dev = sum(dev_ms) / 1e3
@@ -447,10 +624,6 @@ def main():
         tot_dev, tot_wall = float(t[0]), float(t[1])
     value = world * nq * args.steps / tot_dev
     e2e = world * nq * args.steps / tot_wall
-    single_qps = nsingle / (single_ms / 1e3) if single_ms > 0 else None
-    # the one-per-call sample is the first nsingle queries: comparable with the
-    # batch only when every query has the same shape (same k, same kind)
-    uniform = len({(len(q), D >= 0) for q, D in zip(queries, Ds)}) == 1
 
     peak, peak_kind = peaks()
     grow_reads = sums["relax"] / (grow_ms / 1e3) if grow_ms > 0 else None
@@ -458,7 +631,7 @@ def main():
     achieved = gb / (grow_ms / 1e3) / 1e9 if grow_ms > 0 else None
     traffic = None
     tp = os.path.join(ROOT, "profiles", f"grow_{args.workload}_traffic.json")
-    if os.path.exists(tp):
+    if os.path.exists(tp) and unfiltered:
         with open(tp) as f:
             traffic = json.load(f).get("dram_bytes_per_launch")
 
@@ -469,17 +642,21 @@ def main():
         "data": "synthetic (seeded BA power-law graphs standing in for the reference's external datasets)",
         "config": {"workload": WORKLOADS[args.workload], "queries_per_step_per_gpu": nq,
                    **({"query_filter": f"k={args.k or 'any'} kind={args.kind} first={args.queries or 'all'}"}
-                      if (args.k or args.kind != "all" or args.queries) else {}),
+                      if not unfiltered else {}),
                    "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before every step; "
-                   "per-query DP tables (hundreds of MB per step) exceed L2"},
+                   "per-query DP tables (GBs per step) exceed L2"},
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "gpu_launches": launches,
         "single_query_qps": single_qps,
-        "single_query_sample": f"first {nsingle} queries, one per call" if nsingle else None,
-        "batched_over_single": (value / world) / single_qps if single_qps and uniform else None,
+        "single_query_sample": {"per_class": single,
+                                "how": f"first {args.single_per_class} queries of each (k, kind) class, one per "
+                                       "call; classes weighted by their count in the batch"},
+        "batched_over_single": (value / world) / single_qps if single_qps else None,
+        "parity": parity,
         "latency_ms_in_batch": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
-                                "p99": float(np.percentile(lat, 99))},
+                                "p99": float(np.percentile(lat, 99)),
+                                "note": "admission to answer with the whole batch admitted at once"},
         "state_relaxations_per_s": world * sums["relax"] / tot_dev,
         "roofline": {"kernel": "k_grow", "bound": "hbm", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s",
@@ -487,7 +664,8 @@ def main():
                      "algorithmic_bytes_per_launch": gb / max(grow_launches, 1),
                      "avg_launch_ms": grow_ms / max(grow_launches, 1),
                      "grow_share_of_device_time": grow_ms / (tot_dev * 1e3) if tot_dev else None,
-                     "merge_ms": merge_ms,
+                     "merge_ms_per_step": merge_ms / args.steps,
+                     "merge_share_of_device_time": merge_ms / (tot_dev * 1e3) if tot_dev else None,
                      # the grow's target reads are random 4-byte reads: their
                      # rate against a library random gather on the same GPU
                      "random_reads": {"grow_target_reads_per_s": grow_reads,
@@ -495,15 +673,18 @@ def main():
                                       "frac": grow_reads / ceiling["reads_per_s"] if grow_reads else None}},
         "clocks": clocks,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        procs = max(1, min(os.cpu_count() or 1, 16))
-        qps, times, kind, nproc, nsample, k = cpu_reference_sample(wl, args.workload, procs, procs)
-        out["cpu_baseline"] = {
-            "value": qps, "unit": "queries/s", "cores": nproc, "kind": kind,
-            "sample": f"first {nsample} k={k} queries of this workload, {nproc} single-threaded "
-                      f"PrunedDP++ processes on disjoint query ranges (wall clock incl. graph load); "
-                      f"reference-internal time per query median "
-                      f"{statistics.median(times) if times else float('nan'):.3f} s"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and unfiltered:
+        cores = max(1, min(os.cpu_count() or 1, 32))
+        smp = cpu_reference_sample(args.workload, per_k=2)
+        if smp is not None:
+            qps = cpu_mix_qps(smp["per_k_s"], wl.queries, cores)
+            out["cpu_baseline"] = {
+                "value": qps, "unit": "queries/s", "cores": cores, "kind": "reference",
+                "sample": f"the first {smp['per_k']} plain queries of each k of this workload, one "
+                          f"single-threaded PrunedDP++ process each ({smp['queries']} at once); per-query "
+                          f"time from the reference's progress lines (graph load excluded); value = "
+                          f"{cores} cores / the plain-query mix's mean time per query; mean s per query "
+                          "by k: " + ", ".join(f"k={k}: {t:.2f}" for k, t in sorted(smp["per_k_s"].items()))}
     if rank == 0 and args.ref_gpu > 0:
         eng.close()
         torch.cuda.empty_cache()

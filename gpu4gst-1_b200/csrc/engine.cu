@@ -118,6 +118,7 @@ struct Request {
   gst_status status = GST_OK;
   gst_result result{};
   cudaEvent_t t0 = nullptr;
+  std::chrono::steady_clock::time_point t_submit, t_admit;
 };
 
 class Engine {
@@ -268,6 +269,7 @@ class Engine {
   // queues it.  Returns the request.
   std::shared_ptr<Request> make_request(const int32_t* ids, int k, int D, gst_status* st) {
     auto r = std::make_shared<Request>();
+    r->t_submit = r->t_admit = std::chrono::steady_clock::now();
     r->D = D;
     *st = GST_OK;
     if (!ids || k <= 0) { *st = fail(GST_E_INVALID, "query: no group ids"); return nullptr; }
@@ -540,6 +542,7 @@ class Engine {
         break;  // wait for running queries to free memory
       }
       pending_.pop_front();
+      r->t_admit = std::chrono::steady_clock::now();
       Slot& q = h_slot_[t];  // its previous copy finished: the slot was harvested after a sync
       std::memset(&q, 0, sizeof q);
       q.table = sb.table;
@@ -781,6 +784,12 @@ class Engine {
       slot_busy_[t] = 0;
       slot_req_[t] = nullptr;
       --active_;
+      {
+        using ms = std::chrono::duration<double, std::milli>;
+        const auto now = std::chrono::steady_clock::now();
+        res.stats.queue_ms = ms(r->t_admit - r->t_submit).count();
+        res.stats.latency_ms = ms(now - r->t_submit).count();
+      }
       r->done = true;
     }
     cudaEventDestroy(t1);

@@ -143,6 +143,8 @@ typedef struct {
   int64_t merges;       /* merge partner pairs evaluated (past the lower-bound pre-filter) */
   int64_t touched;      /* vertices that held a finite state */
   double device_ms;     /* device time from admission to answer */
+  double queue_ms;      /* host time from submission to admission into a slot */
+  double latency_ms;    /* host time from submission to the result being ready */
 } gst_stats;
 
 typedef struct {
