@@ -45,7 +45,8 @@ DATASETS = {
     "s3000": dict(graph=dict(V=3000, m=4, wmin=1, wmax=100, seed=3, path=True),
                   groups=dict(G=200, seed=4, geometric=[8, 2, 200]),
                   queries=[dict(k=5, n=12, seed=16), dict(k=7, n=6, seed=18)],
-                  hop=[dict(k=5, D=2, n=6), dict(k=5, D=3, n=6)]),
+                  hop=[dict(k=5, D=2, n=6), dict(k=5, D=3, n=6),
+                       dict(k=7, D=2, n=6), dict(k=7, D=3, n=6), dict(k=7, D=4, n=6)]),
     "c1": dict(graph=dict(V=10000, m=5, wmin=1, wmax=100, seed=1, path=False),
                groups=dict(G=500, seed=101, uniform=[2, 20]),
                queries=[dict(k=3, n=50, seed=201)],

@@ -1,0 +1,221 @@
+"""Generates tests/golden/c3.json and c4.json: reference costs at the
+benchmark sizes, from the reference programs themselves.
+
+C3 is the 1M-vertex diameter-bounded k=7 workload (BA m=10, w U[1,1000],
+10,000 groups Geom(10) in [2,500], 300 queries with D in {2..5}); C4 is the
+4M-vertex mixed workload the benchmark's headline is measured on (BA m=9 +
+spanning path, w U[1,100], 20,000 groups Geom(12) in [2,1000], 300 queries,
+k in {3,5,7}, half D-bounded).  Both are regenerated from their seeds by the
+project's generator; the fixtures store the query indices of a seeded subset
+of each (k, D) cell, the queries themselves and the costs the reference
+printed.
+
+The reference programs (oracle/_ref/, built by oracle/Makefile) run as many
+single-threaded processes at once as the cores and a memory budget allow:
+D-PrunedDP++ allocates its whole (vertex, group set, depth) table up front
+(44-byte nodes in nested vectors, code/D-PrunedDP++/include/CPUHOP.h:107-130),
+so its memory is known before it starts.  Cells whose table does not fit
+(C4 k=7 with a diameter bound: 88 to 155 GB) are recorded as not pinned,
+with the reason.  Every finished cell is written to the fixture at once, so
+an interrupted run keeps what it finished and a rerun resumes.
+
+    python tests/golden/make_golden_large.py c4|c3 [--procs N] [--mem-gb G]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "gpu4gst-1_b200"))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+from gst_b200 import datagen as dg  # noqa: E402
+import make_golden as mg  # noqa: E402
+import oracle  # noqa: E402
+
+# Seeded subsets: the first n queries (in workload order) of each (k, D)
+# cell, D = -1 for plain.  n is set by what the reference finishes in
+# reasonable time on a few cores; 0 marks a cell the reference cannot run.
+SUBSETS = {
+    "c4": {(3, -1): 52, (5, -1): 24, (7, -1): 24,
+           (3, 2): 10, (3, 3): 10, (3, 4): 10, (3, 5): 10,
+           (5, 2): 2, (5, 3): 2, (5, 4): 2, (5, 5): 2,
+           (7, 2): 0, (7, 3): 0, (7, 4): 0, (7, 5): 0},
+    "c3": {(7, 2): 6, (7, 3): 6, (7, 4): 3, (7, 5): 3},
+}
+PLAIN_PER_JOB = 4  # plain queries per process (amortises the graph load)
+
+
+def workload(name):
+    if name == "c4":
+        return dg.config_c4(1, n_queries=300), dict(config="c4", seed=1, n_queries=300)
+    if name == "c3":
+        return dg.config_c3(1, n_queries=300), dict(config="c3", seed=1, n_queries=300)
+    raise SystemExit(f"unknown dataset {name}")
+
+
+def mem_bytes(wl, k, D):
+    """Resident memory of one reference process: the graph in its hash and
+    vector forms (measured about 2 GB for C4), plus D-PrunedDP++'s table of
+    V * 2^k * (D+1) nodes of 44 bytes in vectors (24-byte header and a
+    16-byte allocation per (v, set))."""
+    g = 2.5e9 * wl.graph.E / 80e6 + 0.3e9
+    if D < 0:
+        return g
+    return g + wl.graph.V * (1 << k) * (40 + 44 * (D + 1))
+
+
+def run_jobs(jobs, procs, mem_budget, log):
+    """Runs the jobs (dicts with argv, cwd, mem, done) with at most `procs`
+    at once and the sum of their memory within the budget: the first listed
+    job that fits starts, else the loop waits for one to end."""
+    lock = threading.Condition()
+    state = {"mem": 0.0, "run": 0}
+    threads = []
+
+    def work(job):
+        t0 = time.time()
+        try:
+            subprocess.run(job["argv"], check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                           stdin=subprocess.DEVNULL, cwd=job["cwd"])
+            job["wall"] = time.time() - t0
+            job["done"](job)
+        except Exception as e:  # a failed job leaves its cell unfinished
+            log(f"{job['label']}: failed ({e})")
+        finally:
+            with lock:
+                state["mem"] -= job["mem"]
+                state["run"] -= 1
+                lock.notify_all()
+
+    todo = []
+    for job in jobs:
+        if job["mem"] > mem_budget:
+            log(f"skip (needs {job['mem'] / 1e9:.0f} GB): {job['label']}")
+        else:
+            todo.append(job)
+    while todo:
+        with lock:
+            def fits():
+                return [j for j in todo if state["mem"] + j["mem"] <= mem_budget] if state["run"] < procs else []
+            lock.wait_for(lambda: bool(fits()))
+            job = fits()[0]
+            todo.remove(job)
+            state["mem"] += job["mem"]
+            state["run"] += 1
+        th = threading.Thread(target=work, args=(job,))
+        th.start()
+        threads.append(th)
+    for th in threads:
+        th.join()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("name", choices=sorted(SUBSETS))
+    ap.add_argument("--procs", type=int, default=max(1, (os.cpu_count() or 2) - 2))
+    ap.add_argument("--mem-gb", type=float, default=48.0)
+    ap.add_argument("--data-dir", default="", help="reuse a directory holding the written dataset")
+    args = ap.parse_args()
+    name = args.name
+    out_path = os.path.join(HERE, f"{name}.json")
+    wl, spec = workload(name)
+    queries = wl.queries
+    fx = dict(name=name, spec=spec, checksum=mg.checksum(wl.graph, wl.groups), cells=[],
+              generated_by="tests/golden/make_golden_large.py (reference PrunedDP++ / D-PrunedDP++ built "
+                           "from source by oracle/Makefile, one single-threaded process per query range)")
+    if os.path.exists(out_path):  # resume: keep the finished cells of the same inputs
+        with open(out_path) as f:
+            old = json.load(f)
+        if old.get("checksum") == fx["checksum"]:
+            fx["cells"] = [c for c in old.get("cells", []) if c.get("costs") or c.get("not_pinned")]
+    done_cells = {(c["k"], c["D"]) for c in fx["cells"]}
+    wlock = threading.Lock()
+
+    def log(msg):
+        print(time.strftime("%H:%M:%S"), msg, flush=True)
+
+    def save():
+        with wlock:
+            fx["cells"].sort(key=lambda c: (c["D"] >= 0, c["k"], c["D"]))
+            with open(out_path + ".tmp", "w") as f:
+                json.dump(fx, f, indent=1)
+            os.replace(out_path + ".tmp", out_path)
+
+    d = args.data_dir or tempfile.mkdtemp(prefix=f"gstgold_{name}_")
+    if not os.path.exists(os.path.join(d, name + ".in")):
+        dg.write_dataset(d, name, dg.Workload(wl.graph, wl.groups, []), binary=False)
+    os.makedirs(os.path.join(d, "result"), exist_ok=True)
+    log(f"dataset in {d}")
+    jobs = []
+    for (k, D), n in SUBSETS[name].items():
+        if (k, D) in done_cells:
+            continue
+        idx = [i for i, (q, qd) in enumerate(queries) if len(q) == k and qd == D][:n]
+        cell = dict(k=k, D=D, idx=idx, queries=[queries[i][0].tolist() for i in idx])
+        if n == 0:
+            if any(len(q) == k and qd == D for q, qd in queries):
+                need = mem_bytes(wl, k, D) / 1e9
+                cell.update(idx=[], queries=[], costs=None, program=None,
+                            not_pinned=f"D-PrunedDP++ allocates its whole table up front: {need:.0f} GB "
+                                       f"for k={k}, D={D} on {wl.graph.V:,} vertices")
+                fx["cells"].append(cell)
+            continue
+        if not idx:
+            continue
+        # a data name per cell: symlinks to the shared graph and groups, the
+        # cell's queries as <data><k>.csv
+        data = f"{name}_k{k}_" + ("plain" if D < 0 else f"D{D}")
+        for ext in (".in", ".g"):
+            dst = os.path.join(d, data + ext)
+            if not os.path.exists(dst):
+                os.symlink(os.path.join(d, name + ext), dst)
+        dg.write_queries(os.path.join(d, f"{data}{k}.csv"), [queries[i] for i in idx])
+        prog = "PrunedDP++" if D < 0 else "D-PrunedDP++"
+        per = PLAIN_PER_JOB if D < 0 else 1
+        cell.update(costs=[None] * len(idx), ref_time_s=[None] * len(idx), program=prog)
+        pending = {"n": 0}
+        for a in range(0, len(idx), per):
+            b = min(a + per, len(idx)) - 1
+            argv = [oracle.ref_binary(prog), "1" if D < 0 else "2", d + "/", data, str(k)]
+            argv += ([str(D)] if D >= 0 else []) + [str(a), str(b)]
+            tag = "CPU_nonHop" if D < 0 else "CPU_Hop"
+            csv = os.path.join(d, "result", f"exp_{tag}_{data}_T{k}_" + (f"D{D}_" if D >= 0 else "") + f"{a}-{b}.csv")
+            pending["n"] += 1
+
+            def done(job, cell=cell, a=a, csv=csv, pending=pending):
+                with open(csv) as f:
+                    next(f)
+                    rows = [ln.strip().split(",") for ln in f if ln.strip()]
+                with wlock:
+                    for j, r in enumerate(rows):
+                        cell["costs"][a + j] = int(r[3])
+                        cell["ref_time_s"][a + j] = float(r[2])
+                    pending["n"] -= 1
+                    last = pending["n"] == 0
+                    if last:
+                        fx["cells"].append(cell)
+                log(f"{job['label']}: {[r[3] for r in rows]} in {job['wall']:.0f} s")
+                if last:
+                    save()
+
+            jobs.append(dict(argv=argv, cwd=d, mem=mem_bytes(wl, k, D), done=done,
+                             label=f"{name} k={k} D={D} queries {a}-{b}"))
+    save()
+    log(f"{len(jobs)} jobs, {args.procs} processes, {args.mem_gb} GB")
+    run_jobs(jobs, args.procs, args.mem_gb * 1e9, log)
+    save()
+    log("done")
+
+
+if __name__ == "__main__":
+    main()

@@ -106,3 +106,51 @@ def test_c2_equals_the_reference_binaries(golden):
             if r.feasible:
                 assert oracle.validate(g, gr, q, r.edges, r.root, r.cost, h["D"]) == 0
     e.close()
+
+
+def _large_fixture(name):
+    """A reference-pinned fixture at benchmark size (tests/golden/<name>.json,
+    made by tests/golden/make_golden_large.py) and its regenerated inputs."""
+    import json
+    import os
+    import sys
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    path = os.path.join(here, f"{name}.json")
+    if not os.path.exists(path):
+        pytest.skip(f"{path} not generated")
+    with open(path) as f:
+        fx = json.load(f)
+    sys.path.insert(0, here)
+    import make_golden as mg
+    wl = dg.config_c4(1, n_queries=300) if name == "c4" else dg.config_c3(1, n_queries=300)
+    assert mg.checksum(wl.graph, wl.groups) == fx["checksum"], f"{name}: generator no longer reproduces the fixture"
+    cells = [c for c in fx["cells"] if c.get("costs") and all(x is not None for x in c["costs"])]
+    assert cells
+    return fx, wl, cells
+
+
+@pytest.mark.parametrize("name", ["c4", "c3"])
+def test_benchmark_size_costs_equal_the_reference_binaries(name):
+    """C4 (4M vertices, the headline workload) and C3 (1M vertices, k=7 with
+    D in {2..5}): every pinned query of every (k, D) cell equals the cost the
+    reference PrunedDP++ / D-PrunedDP++ printed, solved as one batch; the first
+    query of each cell also one per call; every tree passes the checker."""
+    fx, wl, cells = _large_fixture(name)
+    e = gst_b200.Engine(device=0, max_rounds=2000000)
+    e.load_graph(wl.graph.rowptr, wl.graph.col, wl.graph.w)
+    e.load_groups(wl.groups.ptr, wl.groups.mem)
+    qs, Ds, want = [], [], []
+    for c in cells:
+        for q, cost in zip(c["queries"], c["costs"]):
+            qs.append(q)
+            Ds.append(c["D"])
+            want.append(cost)
+    got = e.solve_batch(qs, Ds)
+    assert [r.cost for r in got] == want
+    for q, D, r in zip(qs, Ds, got):
+        assert r.status == 0
+        if r.feasible:
+            assert oracle.validate(wl.graph, wl.groups, q, r.edges, r.root, r.cost, D) == 0
+    for c in cells:
+        assert e.solve(c["queries"][0], c["D"]).cost == c["costs"][0], (c["k"], c["D"])
+    e.close()
