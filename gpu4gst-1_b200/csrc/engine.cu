@@ -615,7 +615,8 @@ class Engine {
     k_ctl_a<<<1, MAXSLOTS, 0, st>>>(d_slots_, max_slots_, d_plan_, d_status_);
     k_lbprep<<<std::min(max_slots_, 256), 256, 0, st>>>(d_slots_, d_plan_, g);
     if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 0], st, cudaEventRecordExternal);
-    k_merge<<<grid, MERGE_THREADS, 0, st>>>(d_slots_, d_plan_, g);
+    k_merge_t<false><<<grid, MERGE_THREADS, 0, st>>>(d_slots_, d_plan_, g);
+    k_merge_t<true><<<grid, MERGE_THREADS, 0, st>>>(d_slots_, d_plan_, g);
     if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 1], st, cudaEventRecordExternal);
     k_prep<<<grid, 256, 0, st>>>(d_slots_, d_plan_, g);
     k_ctl_b<<<1, MAXSLOTS, 0, st>>>(d_slots_, d_plan_);
@@ -648,7 +649,7 @@ class Engine {
                              cudaMemcpyDeviceToHost, stream_));
     if (gst_status st = wait_stream(); st != GST_OK) return st;
     prof_.rounds += rounds_per_poll_;
-    prof_.kernel_launches += 6 * rounds_per_poll_ + 1;
+    prof_.kernel_launches += 7 * rounds_per_poll_ + 1;
     prof_.d2h_bytes += sizeof(SlotStatus) * max_slots_;
     if (profile_) {
       for (int i = 0; i < rounds_per_poll_; ++i) {

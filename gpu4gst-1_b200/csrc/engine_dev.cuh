@@ -118,6 +118,7 @@ struct SlotStatus {
 
 struct Plan {
   int32_t n_lb, n_merge, n_grow, n_active;
+  int32_t n_wide_merge;  // merging slots with more than 6 labels (k_merge_wide)
   int32_t lb_slots[MAXSLOTS];
   int32_t merge_slots[MAXSLOTS];
   int32_t grow_slots[MAXSLOTS];

@@ -317,6 +317,8 @@ __global__ void k_ctl_a(Slot* slots, int nslots, Plan* plan, SlotStatus* status)
   }
   // compact the slot list of each action with block-wide inclusive scans
   const int f0 = (act == A_LBPREP), f1 = (act == A_MERGE || act == A_MERGEFULL), f2 = (act == A_GROW);
+  const int n_wide = __syncthreads_count(f1 && slots[t < nslots ? t : 0].L > 6);
+  if (t == 0) plan->n_wide_merge = n_wide;
   s_cnt[0][t] = f0;
   s_cnt[1][t] = f1;
   s_cnt[2][t] = f2;
@@ -588,49 +590,36 @@ __device__ __forceinline__ void merge_costs(const int32_t* row, const uint8_t* s
 }
 
 // Returns whether the split loop ran (false: the lower-bound pre-filter
-// rejected the item).
+// rejected the item).  vdist: the vertex's clipped singleton distances and
+// vmiss: the groups with no singleton entry at the vertex, both computed
+// once per vertex by the lanes that share it.
 template <int LT>
 __device__ __forceinline__ bool merge_item(Slot& q, int t, uint32_t v, int r, int S, const uint8_t* sidx,
-                                           int* dist, Graph& g, unsigned long long* ans,
+                                           const int* vdist, unsigned vmiss, Graph& g, unsigned long long* ans,
                                            unsigned long long* dirty0, int* dmin) {
   const int k = q.k, W = q.W, L = LT > 0 ? LT : q.L, rowlen = W * L, D = q.D, s = q.s;
   const bool hop = D >= 0;
   const int lo = c_sub.loff[k][s];
   int32_t* row = q.table + (long long)v * rowlen;
   const int best = *(volatile int*)&q.best;
+  // R1 >= INF / 2: layer 1 ran untruncated (best was still unknown), so a
+  // missing singleton entry means the group is out of reach (for a D-query:
+  // more than D hops away) and every state (v, S) holding it is infinite
+  const bool reach_known = q.R1 >= INF / 2;
   int lbv = 0;
   if (s < k) {
     // a tree rooted at v that covers S reaches every group of S, so its cost
     // is at least max_{i in S} dist_i(v): skip the split loop when even that
     // cannot pass the lower-bound test
+    if (reach_known && (vmiss & (unsigned)S)) return false;
     int need = 0;
-    bool miss = false;  // a group of S has no entry at v
-    for (int i = 0; i < k; ++i) {
-      int dm = INF;
-      for (int l = 0; l < L; ++l) dm = imin(dm, row[(1 + i) * L + l]);
-      dist[i] = clip_dist(dm, q.R1);
-      if ((S >> i) & 1) {
-        need = imax(need, dist[i]);
-        miss |= dm >= INF;
-      }
-    }
-    // R1 >= INF / 2: layer 1 ran untruncated (best was still unknown), so a
-    // missing singleton entry means the group is out of reach (for a
-    // D-query: more than D hops away) and every state (v, S) is infinite
-    if (miss && q.R1 >= INF / 2) return false;
-    lbv = lower_bound(dist, k, W, S, q.lbtab, (long long)best - need);
+    for (int x = S; x; x &= x - 1) need = imax(need, vdist[__ffs(x) - 1]);
+    lbv = lower_bound(vdist, k, W, S, q.lbtab, (long long)best - need);
     if ((long long)need + lbv > best) return false;
   } else {
     // full join: the answer at v is a tree rooted at v touching every group
-    bool miss = false;
-    for (int i = 0; i < k; ++i) {
-      int dm = INF;
-      for (int l = 0; l < L; ++l) dm = imin(dm, row[(1 + i) * L + l]);
-      dist[i] = clip_dist(dm, q.R1);
-      miss |= dm >= INF;
-    }
-    if (miss && q.R1 >= INF / 2) return false;
-    if (full_bound(dist, k, W, q.lbtab) > best) return false;
+    if (reach_known && vmiss) return false;
+    if (full_bound(vdist, k, W, q.lbtab) > best) return false;
   }
   int M[LT > 0 ? LT : MAXL];
   merge_costs<LT>(row, sidx, S, L, D, M);
@@ -670,19 +659,26 @@ __device__ __forceinline__ bool merge_item(Slot& q, int t, uint32_t v, int r, in
 }
 
 // 4 blocks per SM (64 registers, no spills): 25% faster than the 3 that 78
-// registers allow, on C2 and C4
+// registers allow, on C2 and C4.  Label counts up to 6 (D <= 5) are
+// compile-time cases of k_merge; larger ones (D >= 6) run in k_merge_wide,
+// whose run-time label loops need more registers than the kernel of the
+// common cases may use without spilling.  Each kernel skips the other's
+// items; k_merge_wide returns at once when no merging slot needs it.
+template <bool WIDE>
 __global__ void __launch_bounds__(MERGE_THREADS, 4)
-k_merge(Slot* slots, const Plan* plan, Graph g) {
+k_merge_t(Slot* slots, const Plan* plan, Graph g) {
   __shared__ long long s_off[MAXSLOTS + 1];
   __shared__ int s_slot[MAXSLOTS];
   __shared__ uint8_t s_sidx[MAXK + 1][MAXW], s_sof[MAXK + 1][MAXW];
-  // per-thread singleton distances; the lower bound indexes them by set bit,
-  // which would put a register array in local memory.  An odd stride keeps
-  // the lanes of a warp in distinct banks.
-  __shared__ int s_dist[MERGE_THREADS * DIST_STRIDE];
-  int* dist = s_dist + threadIdx.x * DIST_STRIDE;
+  // singleton distances of the vertex whose items start at a lane (the lower
+  // bound indexes them by set bit, which would put a register array in local
+  // memory), and the vertex's unreachable-group mask
+  __shared__ int s_vdist[MERGE_THREADS * DIST_STRIDE];
+  __shared__ unsigned s_vmiss[MERGE_THREADS];
+  const int lane = threadIdx.x & 31;
+  const int wbase = threadIdx.x - lane;
   const int nm = plan->n_merge;
-  if (nm == 0) return;
+  if (nm == 0 || (WIDE && plan->n_wide_merge == 0)) return;
   for (int x = threadIdx.x; x <= nm; x += blockDim.x) s_off[x] = plan->merge_off[x];
   for (int x = threadIdx.x; x < nm; x += blockDim.x) s_slot[x] = plan->merge_slots[x];
   for (int x = threadIdx.x; x < (MAXK + 1) * MAXW; x += blockDim.x) {
@@ -701,34 +697,72 @@ k_merge(Slot* slots, const Plan* plan, Graph g) {
     uint32_t v = 0;
     unsigned long long nsplit = 0;
     int alive = 0;
+    int r = 0;  // rank of the item's set in the layer
     if (gi < total) {
       const int j = seg_search(s_off, nm, gi);
       t = s_slot[j];
       Slot& q = slots[t];
+      if (WIDE == (q.L > 6)) {
+        const int k = q.k, s = q.s;
+        const int nS = c_sub.loff[k][s + 1] - c_sub.loff[k][s];
+        const long long local = gi - s_off[j];
+        const int vi = (int)(local / nS);
+        r = (int)(local % nS);
+        v = vi < q.nlr ? q.live[q.lr][vi] : q.touched[q.mt0 + vi - q.nlr];
+        key = ((unsigned long long)(unsigned)t << 32) | (unsigned)vi;
+      } else {
+        t = -1;  // the other merge kernel's item
+      }
+    }
+    // The items of one vertex are consecutive lanes (a segment of equal key).
+    // Its lanes split the k singleton minima between them (each over the L
+    // labels) and leave them, clipped, in the head lane's shared slot, with
+    // the groups that have no entry in the head's miss mask.
+    const unsigned seg = __match_any_sync(0xffffffffu, key);
+    const int head = __ffs(seg) - 1;
+    const int* vdist = s_vdist + (wbase + head) * DIST_STRIDE;
+    s_vmiss[threadIdx.x] = 0u;
+    __syncwarp();
+    if (t >= 0) {
+      const Slot& q = slots[t];
+      const int k = q.k, L = q.L, R1 = q.R1;
+      const int32_t* row = q.table + (long long)v * ((long long)q.W * L);
+      const int off = __popc(seg & ((1u << lane) - 1)), seglen = __popc(seg);
+      unsigned mm = 0;
+      for (int i = off; i < k; i += seglen) {
+        int dm = INF;
+        for (int l = 0; l < L; ++l) dm = imin(dm, row[(1 + i) * L + l]);
+        s_vdist[(wbase + head) * DIST_STRIDE + i] = clip_dist(dm, R1);
+        if (dm >= INF) mm |= 1u << i;
+      }
+      if (mm) atomicOr(&s_vmiss[wbase + head], mm);
+    }
+    __syncwarp();
+    if (t >= 0) {
+      Slot& q = slots[t];
       const int k = q.k, s = q.s;
-      const int lo = c_sub.loff[k][s], nS = c_sub.loff[k][s + 1] - lo;
-      const long long local = gi - s_off[j];
-      const int vi = (int)(local / nS), r = (int)(local % nS);
-      const int S = s_sof[k][lo + r];
+      const int S = s_sof[k][c_sub.loff[k][s] + r];
       const uint8_t* sidx = s_sidx[k];
-      v = vi < q.nlr ? q.live[q.lr][vi] : q.touched[q.mt0 + vi - q.nlr];
-      key = ((unsigned long long)(unsigned)t << 32) | (unsigned)vi;
+      const unsigned vmiss = s_vmiss[wbase + head];
       bool ev = false;
-      switch (q.L) {
-        case 1: ev = merge_item<1>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
-        case 2: ev = merge_item<2>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
-        case 3: ev = merge_item<3>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
-        case 4: ev = merge_item<4>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
-        case 5: ev = merge_item<5>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
-        case 6: ev = merge_item<6>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
-        default: ev = merge_item<0>(q, t, v, r, S, sidx, dist, g, &ans, &dirty, &dmin); break;
+      if (WIDE) {
+        ev = merge_item<0>(q, t, v, r, S, sidx, vdist, vmiss, g, &ans, &dirty, &dmin);
+      } else {
+        switch (q.L) {
+          case 1: ev = merge_item<1>(q, t, v, r, S, sidx, vdist, vmiss, g, &ans, &dirty, &dmin); break;
+          case 2: ev = merge_item<2>(q, t, v, r, S, sidx, vdist, vmiss, g, &ans, &dirty, &dmin); break;
+          case 3: ev = merge_item<3>(q, t, v, r, S, sidx, vdist, vmiss, g, &ans, &dirty, &dmin); break;
+          case 4: ev = merge_item<4>(q, t, v, r, S, sidx, vdist, vmiss, g, &ans, &dirty, &dmin); break;
+          case 5: ev = merge_item<5>(q, t, v, r, S, sidx, vdist, vmiss, g, &ans, &dirty, &dmin); break;
+          default: ev = merge_item<6>(q, t, v, r, S, sidx, vdist, vmiss, g, &ans, &dirty, &dmin); break;
+        }
       }
       if (ev) nsplit = (1ull << (__popc(S) - 1)) - 1;
       // the vertex stays on the next layer's list while a tree through it
       // can still cost <= best (best only falls, so a dropped vertex never
-      // returns); dist holds its singleton distances (computed for s < k)
+      // returns)
       if (r == 0 && s < k && q.D < 0) {
-        alive = full_bound(dist, k, q.W, q.lbtab) <= *(volatile int*)&q.best;
+        alive = full_bound(vdist, k, q.W, q.lbtab) <= *(volatile int*)&q.best;
         if (!alive) atomicOr(&q.dead[v >> 5], 1u << (v & 31));
       }
     }

@@ -297,7 +297,8 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
     for (int r = 0; r < 8; ++r) {
       k_ctl_a<<<1, MAXSLOTS, 0, s>>>(d_slot, 1, d_plan, d_status);
       k_lbprep<<<1, 256, 0, s>>>(d_slot, d_plan, g);
-      k_merge<<<grid, MERGE_THREADS, 0, s>>>(d_slot, d_plan, g);
+      k_merge_t<false><<<grid, MERGE_THREADS, 0, s>>>(d_slot, d_plan, g);
+      k_merge_t<true><<<grid, MERGE_THREADS, 0, s>>>(d_slot, d_plan, g);
       k_prep<<<grid, 256, 0, s>>>(d_slot, d_plan, g);
       k_ctl_b<<<1, MAXSLOTS, 0, s>>>(d_slot, d_plan);
       k_grow<<<grid, GROW_WARPS * 32, 0, s>>>(d_slot, d_plan, g);
