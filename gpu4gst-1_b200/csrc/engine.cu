@@ -684,8 +684,9 @@ class Engine {
       std::memcpy(h_list_, wit.data(), sizeof(int) * wit.size());
       GST_CUDA(cudaMemcpyAsync(d_list_, h_list_, sizeof(int) * wit.size(), cudaMemcpyHostToDevice, stream_));
       k_witness<<<(int)wit.size(), 256, 0, stream_>>>(d_slots_, d_list_, (int)wit.size(), g);
+      k_validate<<<(int)wit.size(), 256, 0, stream_>>>(d_slots_, d_list_, (int)wit.size(), g);
       GST_CUDA(cudaGetLastError());
-      prof_.kernel_launches += 1;
+      prof_.kernel_launches += 2;
       prof_.h2d_bytes += sizeof(int) * wit.size();
     }
     // one read-back of the slot array, then one batch of tree-edge copies
@@ -733,9 +734,15 @@ class Engine {
       if (q.phase == PH_ERROR || q.err != ERR_NONE) {
         static const char* why[] = {"", "chunk list overflow", "frontier list overflow",
                                     "tree reconstruction failed", "tree reconstruction buffer overflow",
-                                    "round limit exceeded"};
-        r->status = fail(GST_E_LIMIT,
-                         std::string("device: ") + (q.err >= 0 && q.err <= 5 ? why[q.err] : "error"));
+                                    "round limit exceeded", "tree check failed"};
+        static const char* tree_why[] = {"", "an edge is not in the graph with that weight",
+                                         "an edge is listed twice", "the edges are not one tree",
+                                         "a queried group has no vertex in the tree",
+                                         "the edge weights do not sum to the cost",
+                                         "hop diameter above D", "tree larger than the check's scratch"};
+        std::string msg = std::string("device: ") + (q.err >= 0 && q.err <= 6 ? why[q.err] : "error");
+        if (q.err == ERR_TREE && q.terr > 0 && q.terr <= 7) msg += std::string(": ") + tree_why[q.terr];
+        r->status = fail(GST_E_LIMIT, msg);
         res.cost = GST_REF_INF;
       } else if ((q.answer >> 32) >= (unsigned long long)INF) {
         res.cost = GST_REF_INF;
@@ -744,24 +751,18 @@ class Engine {
         res.cost = (int64_t)(q.answer >> 32);
         res.feasible = 1;
         res.root = (int32_t)(q.answer & 0xffffffffu);
+        // k_validate checked the edges (distinct, a tree of the cost's weight)
         const int ne = q.nwedges;
         const int32_t* e = h_wedges_ + woff[fi];
-        // the derivation may list an edge twice; report each edge once
-        std::set<std::pair<int, int>> seen;
-        std::vector<int32_t> uniq;
-        for (int x = 0; x < ne; ++x) {
-          int a = e[3 * x], b = e[3 * x + 1];
-          if (seen.insert({std::min(a, b), std::max(a, b)}).second) {
-            uniq.push_back(std::min(a, b));
-            uniq.push_back(std::max(a, b));
-            uniq.push_back(e[3 * x + 2]);
-          }
-        }
-        res.n_edges = (int32_t)(uniq.size() / 3);
+        res.n_edges = ne;
         res.edges = nullptr;
-        if (res.n_edges) {
-          res.edges = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * uniq.size()));
-          std::memcpy(res.edges, uniq.data(), sizeof(int32_t) * uniq.size());
+        if (ne) {
+          res.edges = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * 3 * (size_t)ne));
+          for (int x = 0; x < ne; ++x) {
+            res.edges[3 * x] = std::min(e[3 * x], e[3 * x + 1]);
+            res.edges[3 * x + 1] = std::max(e[3 * x], e[3 * x + 1]);
+            res.edges[3 * x + 2] = e[3 * x + 2];
+          }
         }
         r->status = GST_OK;
       }

@@ -54,7 +54,19 @@ enum Err : int32_t {
   ERR_QUEUE_CAP = 2,
   ERR_WITNESS = 3,
   ERR_WITNESS_CAP = 4,
-  ERR_ROUNDS = 5
+  ERR_ROUNDS = 5,
+  ERR_TREE = 6  // the device check of the returned tree failed (reason in Slot::terr)
+};
+// Reasons of ERR_TREE (Slot::terr).
+enum TreeErr : int32_t {
+  TE_NONE = 0,
+  TE_EDGE = 1,      // an edge is not in the graph or has another weight
+  TE_REPEAT = 2,    // the derivation lists an edge twice
+  TE_SHAPE = 3,     // the edges do not form one tree (cycle or disconnected)
+  TE_COVER = 4,     // a queried group has no vertex in the tree
+  TE_WEIGHT = 5,    // the edge weights do not sum to the cost
+  TE_DIAMETER = 6,  // hop diameter above D
+  TE_SCRATCH = 7    // the tree does not fit the check's scratch
 };
 
 struct Chunk {
@@ -89,6 +101,7 @@ struct Slot {
   int32_t best; // upper bound: cost of a known feasible solution
   int32_t R1;   // singleton distances above R1 are only known to exceed R1
   int32_t err;
+  int32_t terr;  // TreeErr of ERR_TREE
   int32_t ntouched, nchunks, nwedges;
   int32_t rounds;
   // cost-ordered grows (plain problem): states below the bucket bound T are

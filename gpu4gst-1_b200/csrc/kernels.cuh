@@ -1278,6 +1278,145 @@ __global__ void k_witness(Slot* slots, const int* list, int n, Graph g) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Tree check of a finished slot (one block per slot, after k_witness): the
+// witness edges must exist in the graph with their weights, be distinct, form
+// one tree containing the root, touch every queried group, weigh exactly the
+// answer's cost and, with a bound D, have hop diameter <= D.  A failure sets
+// ERR_TREE and the reason, so the query fails instead of returning a tree the
+// engine has not checked (the reference's check, this_is_a_feasible_solution
+// of code/PrunedDP++/include/exp_CPU_nonHop.h:17-49, covers connectivity and
+// groups only).  Scratch: the witness stack, idle once the walk is done.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void tree_fail(Slot& q, int why) {
+  if (atomicCAS(&q.terr, TE_NONE, why) == TE_NONE) q.err = ERR_TREE;
+}
+
+// Hop distances from entry `src` over the tree edges (entries are edge
+// endpoints as representative indices); returns with dist filled (INF where
+// unreachable).  Bellman-Ford rounds: a tree of n edges settles in <= n + 1.
+__device__ void tree_bfs(const int* rep, int ne, int nent, int src, int* dist, int* s_changed) {
+  for (int a = threadIdx.x; a < nent; a += blockDim.x) dist[a] = INF;
+  __syncthreads();
+  if (threadIdx.x == 0) dist[src] = 0;
+  __syncthreads();
+  for (int it = 0; it <= ne + 1; ++it) {
+    if (threadIdx.x == 0) *s_changed = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+      const int a = rep[1 + 2 * i], b = rep[2 + 2 * i];
+      const int da = dist[a], db = dist[b];
+      if (da < INF && da + 1 < db) { atomicMin(&dist[b], da + 1); *s_changed = 1; }
+      if (db < INF && db + 1 < da) { atomicMin(&dist[a], db + 1); *s_changed = 1; }
+    }
+    __syncthreads();
+    const int ch = *s_changed;
+    __syncthreads();
+    if (!ch) break;
+  }
+}
+
+__global__ void k_validate(Slot* slots, const int* list, int n, Graph g) {
+  __shared__ int s_skip, s_changed, s_nv, s_far, s_maxd, s_found, s_ok;
+  __shared__ long long s_sum;
+  for (int j = blockIdx.x; j < n; j += gridDim.x) {
+    __syncthreads();  // the previous slot's shared values are read
+    Slot& q = slots[list[j]];
+    const int ne = q.nwedges;
+    const int nent = 2 * ne + 1;
+    if (threadIdx.x == 0) {
+      s_skip = q.err != ERR_NONE;
+      if (!s_skip && 3ll * nent > 4ll * q.wcap) { tree_fail(q, TE_SCRATCH); s_skip = 1; }
+      s_sum = 0;
+      s_nv = 0;
+      s_maxd = 0;
+      s_far = 0;
+    }
+    __syncthreads();
+    if (s_skip) continue;
+    const int32_t* e = q.wedges;
+    const uint32_t root = (uint32_t)(q.answer & 0xffffffffu);
+    const long long cost = (long long)(q.answer >> 32);
+    int* ent = q.wstack;      // entry 0: the root; 1 + 2i, 2 + 2i: the ends of edge i
+    int* rep = ent + nent;    // first entry holding the same vertex
+    int* dist = rep + nent;   // hop distances, by representative entry
+    for (int a = threadIdx.x; a < nent; a += blockDim.x) ent[a] = a == 0 ? (int)root : e[3 * ((a - 1) >> 1) + ((a - 1) & 1)];
+    __syncthreads();
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+      const int u = e[3 * i], v = e[3 * i + 1], w = e[3 * i + 2];
+      atomicAdd((unsigned long long*)&s_sum, (unsigned long long)(long long)w);
+      for (int i2 = 0; i2 < i; ++i2) {
+        const int u2 = e[3 * i2], v2 = e[3 * i2 + 1];
+        if ((u2 == u && v2 == v) || (u2 == v && v2 == u)) { tree_fail(q, TE_REPEAT); break; }
+      }
+      // scan the shorter of the two adjacency rows (both directions are stored)
+      bool ok = u >= 0 && v >= 0 && u < g.V && v < g.V && u != v;
+      if (ok) {
+        const long long du = g.rowptr[u + 1] - g.rowptr[u], dv = g.rowptr[v + 1] - g.rowptr[v];
+        const int a = du <= dv ? u : v, b = du <= dv ? v : u;
+        bool hit = false;
+        for (long long x = g.rowptr[a]; x < g.rowptr[a + 1] && !hit; ++x) {
+          const int2 aw = g.adj[x];
+          hit = aw.x == b && aw.y == w;
+        }
+        ok = hit;
+      }
+      if (!ok) tree_fail(q, TE_EDGE);
+    }
+    for (int a = threadIdx.x; a < nent; a += blockDim.x) {
+      int r = a;
+      for (int b = 0; b < a; ++b)
+        if (ent[b] == ent[a]) { r = b; break; }
+      rep[a] = r;
+      if (r == a) atomicAdd(&s_nv, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_sum != cost) tree_fail(q, TE_WEIGHT);
+    // n distinct edges on n + 1 vertices, all reachable from the root: a tree
+    if (threadIdx.x == 0 && s_nv != ne + 1) tree_fail(q, TE_SHAPE);
+    tree_bfs(rep, ne, nent, 0, dist, &s_changed);
+    for (int a = threadIdx.x; a < nent; a += blockDim.x) {
+      if (rep[a] != a) continue;
+      if (dist[a] >= INF) tree_fail(q, TE_SHAPE);
+      else atomicMax(&s_maxd, dist[a]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_ok = q.D >= 0 && q.terr == TE_NONE;
+    __syncthreads();
+    if (s_ok) {
+      // the farthest vertex from any vertex ends a longest path of a tree
+      int far = 0;
+      if (threadIdx.x == 0) {
+        for (int a = 0; a < nent; ++a)
+          if (rep[a] == a && dist[a] == s_maxd) { far = a; break; }
+        s_far = far;
+        s_maxd = 0;
+      }
+      __syncthreads();
+      far = s_far;
+      tree_bfs(rep, ne, nent, far, dist, &s_changed);
+      for (int a = threadIdx.x; a < nent; a += blockDim.x)
+        if (rep[a] == a && dist[a] < INF) atomicMax(&s_maxd, dist[a]);
+      __syncthreads();
+      if (threadIdx.x == 0 && s_maxd > q.D) tree_fail(q, TE_DIAMETER);
+    }
+    // every queried group has a member among the tree's vertices
+    for (int i = 0; i < q.k; ++i) {
+      if (threadIdx.x == 0) s_found = 0;
+      __syncthreads();
+      const long long gb = g.gptr[q.groups[i]], ge = g.gptr[q.groups[i] + 1];
+      for (long long m = gb + threadIdx.x; m < ge && !s_found; m += blockDim.x) {
+        const int mv = g.gmem[m];
+        for (int a = 0; a < nent; ++a)
+          if (rep[a] == a && ent[a] == mv) { s_found = 1; break; }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0 && !s_found) tree_fail(q, TE_COVER);
+    }
+    __syncthreads();
+  }
+}
+
 // Publishes every slot's status after a batch of rounds.  A slot whose full
 // merge ran in the last round is finished here (the transition the next
 // control pass would make).
