@@ -870,6 +870,19 @@ extern "C" {
 
 const char* gst_last_error(void) { return gst::last_error_text().c_str(); }
 
+int64_t gst_sizeof(const char* type_name) {
+  if (!type_name) return -1;
+  const std::string n(type_name);
+  if (n == "gst_result") return (int64_t)sizeof(gst_result);
+  if (n == "gst_stats") return (int64_t)sizeof(gst_stats);
+  if (n == "gst_engine_config") return (int64_t)sizeof(gst_engine_config);
+  if (n == "gst_profile") return (int64_t)sizeof(gst_profile);
+  if (n == "gst_csr") return (int64_t)sizeof(gst_csr);
+  if (n == "gst_groups") return (int64_t)sizeof(gst_groups);
+  if (n == "gst_queries") return (int64_t)sizeof(gst_queries);
+  return -1;
+}
+
 gst_status gst_engine_create(const gst_engine_config* cfg, gst_engine** out) {
   if (!out) return gst::fail(GST_E_INVALID, "gst_engine_create: null out");
   *out = nullptr;

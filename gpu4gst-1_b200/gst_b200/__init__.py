@@ -34,7 +34,7 @@ EXPORTS = [
     "gst_read_queries", "gst_csr_free", "gst_groups_free", "gst_queries_free",
     "gst_engine_create", "gst_engine_destroy", "gst_engine_load_graph", "gst_engine_load_groups",
     "gst_result_free", "gst_solve", "gst_solve_batch", "gst_server_start", "gst_server_submit",
-    "gst_server_wait", "gst_server_stop", "gst_engine_profile", "gst_solve_noalloc",
+    "gst_server_wait", "gst_server_stop", "gst_engine_profile", "gst_solve_noalloc", "gst_sizeof",
 ]
 
 
@@ -131,6 +131,16 @@ def load_library() -> ctypes.CDLL:
                  "gst_engine_create", "gst_engine_load_graph", "gst_engine_load_groups", "gst_solve",
                  "gst_solve_batch", "gst_server_start", "gst_server_submit", "gst_server_wait"):
         getattr(lib, name).restype = ctypes.c_int
+    lib.gst_sizeof.argtypes = [ctypes.c_char_p]
+    lib.gst_sizeof.restype = ctypes.c_int64
+    # the structs below must be laid out as the library was compiled
+    for cname, py in (("gst_result", _Result), ("gst_stats", _Stats), ("gst_engine_config", _Config),
+                      ("gst_profile", _Profile), ("gst_csr", _Csr), ("gst_groups", _Groups),
+                      ("gst_queries", _Queries)):
+        n = lib.gst_sizeof(cname.encode())
+        if n != ctypes.sizeof(py):
+            raise RuntimeError(f"{LIB_PATH}: sizeof({cname}) is {n}, the binding expects "
+                               f"{ctypes.sizeof(py)}; rebuild the library")
     _lib = lib
     return lib
 

@@ -41,6 +41,13 @@ typedef enum {
 /* Text of the last error raised on the calling thread (never NULL). */
 const char* gst_last_error(void);
 
+/* sizeof of a public struct of this header as the library was compiled
+ * ("gst_result", "gst_stats", "gst_engine_config", "gst_profile", "gst_csr",
+ * "gst_groups", "gst_queries"), -1 for another name.  Lets a binding check
+ * that it lays the structs out as the library does.  No reference
+ * counterpart. */
+int64_t gst_sizeof(const char* type_name);
+
 /* ---------------------------------------------------------------------------
  * Host-side inputs in the reference's formats
  * ------------------------------------------------------------------------- */
