@@ -144,9 +144,21 @@ class Engine {
     GST_CUDA(cudaGetDeviceProperties(&prop, device_));
     num_sms_ = prop.multiProcessorCount;
     {  // the grow kernel runs one resident wave: grid = SMs x resident blocks
-      int per_sm = 0;
-      GST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grow, GROW_WARPS * 32, 0));
-      grow_grid_ = num_sms_ * std::max(per_sm, 1);
+      int a = 0, b = 0, c3 = 0;
+      GST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_grow_t<8>, GROW_WARPS * 32, 0));
+      GST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_grow_t<16>, GROW_WARPS * 32, 0));
+      GST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c3, k_grow_t<32>, GROW_WARPS * 32, 0));
+      grow_grid_[0] = num_sms_ * std::max(a, 1);
+      grow_grid_[1] = num_sms_ * std::max(b, 1);
+      grow_grid_[2] = num_sms_ * std::max(c3, 1);
+    }
+    std::memset(&tuning_, 0, sizeof tuning_);
+    tuning_.grow_lanes = GROW_LANES_DEFAULT;
+    tuning_.rounds_per_poll = rounds_per_poll_;
+    tuning_.max_slots = max_slots_;
+    for (int k = 0; k <= MAXK; ++k) {
+      tuning_.chunk_pairs[k][0] = tuning_.chunk_pairs[k][1] = 1024;
+      tuning_.bucket_mult[k] = 1;
     }
     GST_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     SubsetTables st;
@@ -338,6 +350,32 @@ class Engine {
   }
 
   gst_profile profile() const { return prof_; }
+
+  gst_status set_tuning(const gst_tuning& t) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (busy_) return fail(GST_E_STATE, "tuning: engine is serving");
+    if (t.grow_lanes && t.grow_lanes != 8 && t.grow_lanes != 16 && t.grow_lanes != 32)
+      return fail(GST_E_INVALID, "tuning: grow_lanes must be 8, 16 or 32");
+    if (t.rounds_per_poll < 0 || t.max_slots < 0 || t.max_slots > MAXSLOTS)
+      return fail(GST_E_INVALID, "tuning: rounds_per_poll or max_slots out of range");
+    for (int k = 0; k <= MAXK; ++k) {
+      if (t.chunk_pairs[k][0] < 0 || t.chunk_pairs[k][1] < 0 || t.chunk_pairs[k][0] > (1 << 20) ||
+          t.chunk_pairs[k][1] > (1 << 20) || t.bucket_mult[k] < 0 || t.bucket_mult[k] > (1 << 16))
+        return fail(GST_E_INVALID, "tuning: chunk_pairs or bucket_mult out of range");
+    }
+    if (t.grow_lanes) tuning_.grow_lanes = t.grow_lanes;
+    if (t.rounds_per_poll) tuning_.rounds_per_poll = rounds_per_poll_ = t.rounds_per_poll;
+    if (t.max_slots) tuning_.max_slots = max_slots_ = t.max_slots;
+    for (int k = 0; k <= MAXK; ++k) {
+      for (int h = 0; h < 2; ++h)
+        if (t.chunk_pairs[k][h]) tuning_.chunk_pairs[k][h] = t.chunk_pairs[k][h];
+      if (t.bucket_mult[k]) tuning_.bucket_mult[k] = t.bucket_mult[k];
+    }
+    drop_graph_exec();  // the captured rounds hold the old launch shapes
+    return GST_OK;
+  }
+
+  gst_tuning tuning() const { return tuning_; }
 
   // One scheduling step: admit, run rounds_per_poll rounds, harvest.
   gst_status step() {
@@ -574,8 +612,9 @@ class Engine {
       q.best = INF;
       q.R1 = INF / 2;
       q.answer = ~0ull;
-      q.delta = delta_;  // plain: first bucket opens at the seeds (cost 0)
+      q.delta = delta_ * tuning_.bucket_mult[k];  // plain: first bucket opens at the seeds (cost 0)
       q.bshift = bucket_shift_;
+      q.chunk_pairs = tuning_.chunk_pairs[k][r->D >= 0 ? 1 : 0];
       q.T = 0;
       q.next_min = INF;
       q.fcur = 2;
@@ -619,9 +658,13 @@ class Engine {
     k_merge_t<true><<<grid, MERGE_THREADS, 0, st>>>(d_slots_, d_plan_, g);
     if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 1], st, cudaEventRecordExternal);
     k_prep<<<grid, 256, 0, st>>>(d_slots_, d_plan_, g);
-    k_ctl_b<<<1, MAXSLOTS, 0, st>>>(d_slots_, d_plan_);
+    k_ctl_b<<<1, MAXSLOTS, 0, st>>>(d_slots_, d_plan_, 32 / tuning_.grow_lanes);
     if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 2], st, cudaEventRecordExternal);
-    k_grow<<<grow_grid_, GROW_WARPS * 32, 0, st>>>(d_slots_, d_plan_, g);
+    switch (tuning_.grow_lanes) {
+      case 8: k_grow_t<8><<<grow_grid_[0], GROW_WARPS * 32, 0, st>>>(d_slots_, d_plan_, g); break;
+      case 32: k_grow_t<32><<<grow_grid_[2], GROW_WARPS * 32, 0, st>>>(d_slots_, d_plan_, g); break;
+      default: k_grow_t<16><<<grow_grid_[1], GROW_WARPS * 32, 0, st>>>(d_slots_, d_plan_, g); break;
+    }
     if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 3], st, cudaEventRecordExternal);
   }
 
@@ -801,7 +844,8 @@ class Engine {
 
   int device_ = -1;
   int num_sms_ = 0;
-  int grow_grid_ = 0;
+  int grow_grid_[3] = {0, 0, 0};  // one resident wave of k_grow_t<8 / 16 / 32>
+  gst_tuning tuning_{};
   int max_slots_ = 256;
   int rounds_per_poll_ = 8;
   cudaStream_t stream_ = nullptr;
@@ -877,6 +921,7 @@ int64_t gst_sizeof(const char* type_name) {
   if (n == "gst_stats") return (int64_t)sizeof(gst_stats);
   if (n == "gst_engine_config") return (int64_t)sizeof(gst_engine_config);
   if (n == "gst_profile") return (int64_t)sizeof(gst_profile);
+  if (n == "gst_tuning") return (int64_t)sizeof(gst_tuning);
   if (n == "gst_csr") return (int64_t)sizeof(gst_csr);
   if (n == "gst_groups") return (int64_t)sizeof(gst_groups);
   if (n == "gst_queries") return (int64_t)sizeof(gst_queries);
@@ -907,6 +952,17 @@ gst_status gst_engine_load_graph(gst_engine* e, int64_t V, const int64_t* rowptr
 gst_status gst_engine_load_groups(gst_engine* e, int64_t n, const int64_t* ptr, const int32_t* members) {
   if (!e) return gst::fail(GST_E_INVALID, "null engine");
   return e->eng.load_groups(n, ptr, members);
+}
+
+gst_status gst_engine_set_tuning(gst_engine* e, const gst_tuning* t) {
+  if (!e || !t) return gst::fail(GST_E_INVALID, "gst_engine_set_tuning: null argument");
+  return e->eng.set_tuning(*t);
+}
+
+gst_status gst_engine_get_tuning(gst_engine* e, gst_tuning* out) {
+  if (!e || !out) return gst::fail(GST_E_INVALID, "gst_engine_get_tuning: null argument");
+  *out = e->eng.tuning();
+  return GST_OK;
 }
 
 gst_status gst_engine_profile(gst_engine* e, gst_profile* out) {

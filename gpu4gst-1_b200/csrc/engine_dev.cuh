@@ -109,6 +109,7 @@ struct Slot {
   // (next_min = their smallest cost) until the near lists run dry; farround
   // marks a round that drains the previous far list
   int32_t delta, bshift, T, next_min, fcur, farround;
+  int32_t chunk_pairs;  // (edge, set) pairs per grow chunk
   int32_t qcount[MAXQ];
   // merge lists: layer s visits live[lr][0, nlr) and touched[mt0, mt1) (the
   // vertices first touched since the previous list was cut) and appends the

@@ -46,10 +46,10 @@ constexpr int GROW_WARPS = 8;
 // (measured best; 6 blocks at 40 registers spill onto the loop).
 constexpr int GROW_MIN_BLOCKS = 4;
 constexpr int GROW_QUEUE = 128;  // improving candidates queued per warp
-// Lanes per chunk: a warp relaxes 32 / GROW_LANES chunks side by side, so
+// Lanes per chunk (a template parameter of k_grow_t: 8, 16 or 32; 16 unless
+// a tuning says otherwise): a warp relaxes 32 / lanes chunks side by side, so
 // the per-chunk latency (descriptor, source row, dirty sets) overlaps.
-constexpr int GROW_LANES = 16;
-constexpr int GROW_CPW = 32 / GROW_LANES;  // chunks per warp
+constexpr int GROW_LANES_DEFAULT = 16;
 
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
@@ -358,7 +358,7 @@ __global__ void k_ctl_a(Slot* slots, int nslots, Plan* plan, SlotStatus* status)
 }
 
 // Chunk offsets of the grow slots, after the prep pass.
-__global__ void k_ctl_b(Slot* slots, Plan* plan) {
+__global__ void k_ctl_b(Slot* slots, Plan* plan, int cpw) {
   __shared__ long long s_scan[MAXSLOTS];
   const int t = threadIdx.x;
   const int n = plan->n_grow;
@@ -367,7 +367,7 @@ __global__ void k_ctl_b(Slot* slots, Plan* plan) {
     Slot& q = slots[plan->grow_slots[t]];
     c = q.nchunks;
     if (c > q.chunk_cap) { q.err = ERR_CHUNK_CAP; c = 0; }
-    c = (c + GROW_CPW - 1) / GROW_CPW;  // grow units: GROW_CPW chunks each
+    c = (c + cpw - 1) / cpw;  // grow units: cpw chunks each (one warp)
   }
   s_scan[t] = c;
   __syncthreads();
@@ -889,7 +889,7 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
           ee = g.rowptr[v + 1];
           nb = __popcll(m);
           if (ee > eb) {
-            ch = imax(32, 1024 / nb);
+            ch = imax(32, q.chunk_pairs / nb);
             nch = (int)((ee - eb + ch - 1) / ch);
           }
         }
@@ -1014,8 +1014,10 @@ __device__ __forceinline__ int grow_improve(Slot& q, long long V, uint32_t u, in
   return 1;
 }
 
+template <int GROW_LANES>
 __global__ void __launch_bounds__(GROW_WARPS * 32, GROW_MIN_BLOCKS)
-k_grow(Slot* slots, const Plan* plan, Graph g) {
+k_grow_t(Slot* slots, const Plan* plan, Graph g) {
+  constexpr int GROW_CPW = 32 / GROW_LANES;  // chunks per warp
   __shared__ long long s_off[MAXSLOTS + 1];
   __shared__ int s_slot[MAXSLOTS];
   __shared__ int s_r[GROW_WARPS][GROW_CPW * 64];

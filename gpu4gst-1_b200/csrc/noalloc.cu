@@ -259,6 +259,7 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   q.answer = ~0ull;
   q.delta = 1;  // replaced on the device by k_delta_set before the first round
   q.bshift = 30;
+  q.chunk_pairs = 1024;
   q.T = 0;
   q.next_min = INF;
   q.fcur = 2;
@@ -300,8 +301,8 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
       k_merge_t<false><<<grid, MERGE_THREADS, 0, s>>>(d_slot, d_plan, g);
       k_merge_t<true><<<grid, MERGE_THREADS, 0, s>>>(d_slot, d_plan, g);
       k_prep<<<grid, 256, 0, s>>>(d_slot, d_plan, g);
-      k_ctl_b<<<1, MAXSLOTS, 0, s>>>(d_slot, d_plan);
-      k_grow<<<grid, GROW_WARPS * 32, 0, s>>>(d_slot, d_plan, g);
+      k_ctl_b<<<1, MAXSLOTS, 0, s>>>(d_slot, d_plan, 32 / GROW_LANES_DEFAULT);
+      k_grow_t<GROW_LANES_DEFAULT><<<grid, GROW_WARPS * 32, 0, s>>>(d_slot, d_plan, g);
     }
     rounds += 8;
     k_publish<<<1, 32, 0, s>>>(d_slot, 1, d_status);

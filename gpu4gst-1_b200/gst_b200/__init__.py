@@ -35,6 +35,7 @@ EXPORTS = [
     "gst_engine_create", "gst_engine_destroy", "gst_engine_load_graph", "gst_engine_load_groups",
     "gst_result_free", "gst_solve", "gst_solve_batch", "gst_server_start", "gst_server_submit",
     "gst_server_wait", "gst_server_stop", "gst_engine_profile", "gst_solve_noalloc", "gst_sizeof",
+    "gst_engine_set_tuning", "gst_engine_get_tuning",
 ]
 
 
@@ -71,6 +72,11 @@ class _Profile(ctypes.Structure):
                 ("grow_launches", ctypes.c_int64), ("merge_ms", ctypes.c_double),
                 ("merge_launches", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
                 ("rounds", ctypes.c_int64), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64)]
+
+
+class _Tuning(ctypes.Structure):
+    _fields_ = [("grow_lanes", ctypes.c_int), ("rounds_per_poll", ctypes.c_int), ("max_slots", ctypes.c_int),
+                ("chunk_pairs", (ctypes.c_int * 2) * (MAX_K + 1)), ("bucket_mult", ctypes.c_int * (MAX_K + 1))]
 
 
 class _Stats(ctypes.Structure):
@@ -123,6 +129,10 @@ def load_library() -> ctypes.CDLL:
                                       ctypes.c_int, ctypes.c_int, P, ctypes.POINTER(ctypes.c_int64),
                                       ctypes.POINTER(ctypes.c_int32)]
     lib.gst_solve_noalloc.restype = ctypes.c_int
+    lib.gst_engine_set_tuning.argtypes = [P, ctypes.POINTER(_Tuning)]
+    lib.gst_engine_set_tuning.restype = ctypes.c_int
+    lib.gst_engine_get_tuning.argtypes = [P, ctypes.POINTER(_Tuning)]
+    lib.gst_engine_get_tuning.restype = ctypes.c_int
     lib.gst_engine_profile.argtypes = [P, ctypes.POINTER(_Profile)]
     lib.gst_engine_profile.restype = ctypes.c_int
     lib.gst_server_stop.argtypes = [P]
@@ -135,7 +145,7 @@ def load_library() -> ctypes.CDLL:
     lib.gst_sizeof.restype = ctypes.c_int64
     # the structs below must be laid out as the library was compiled
     for cname, py in (("gst_result", _Result), ("gst_stats", _Stats), ("gst_engine_config", _Config),
-                      ("gst_profile", _Profile), ("gst_csr", _Csr), ("gst_groups", _Groups),
+                      ("gst_profile", _Profile), ("gst_tuning", _Tuning), ("gst_csr", _Csr), ("gst_groups", _Groups),
                       ("gst_queries", _Queries)):
         n = lib.gst_sizeof(cname.encode())
         if n != ctypes.sizeof(py):
@@ -303,6 +313,29 @@ class Engine:
         p = _Profile()
         _check(self._lib.gst_engine_profile(self._h, ctypes.byref(p)), "profile")
         return {f: getattr(p, f) for f, _ in _Profile._fields_}
+
+    def get_tuning(self) -> dict:
+        """Launch and scheduling parameters (gst_tuning) as a dict:
+        grow_lanes, rounds_per_poll, max_slots, chunk_pairs[k] = [plain, D],
+        bucket_mult[k]."""
+        t = _Tuning()
+        _check(self._lib.gst_engine_get_tuning(self._h, ctypes.byref(t)), "get_tuning")
+        return {"grow_lanes": t.grow_lanes, "rounds_per_poll": t.rounds_per_poll, "max_slots": t.max_slots,
+                "chunk_pairs": [[t.chunk_pairs[k][0], t.chunk_pairs[k][1]] for k in range(MAX_K + 1)],
+                "bucket_mult": [t.bucket_mult[k] for k in range(MAX_K + 1)]}
+
+    def set_tuning(self, tuning: dict) -> None:
+        """Sets the parameters present in `tuning` (same keys as get_tuning;
+        absent or 0 keeps the current value)."""
+        t = _Tuning()
+        t.grow_lanes = int(tuning.get("grow_lanes", 0))
+        t.rounds_per_poll = int(tuning.get("rounds_per_poll", 0))
+        t.max_slots = int(tuning.get("max_slots", 0))
+        for k, pair in enumerate(tuning.get("chunk_pairs", [])[: MAX_K + 1]):
+            t.chunk_pairs[k][0], t.chunk_pairs[k][1] = int(pair[0]), int(pair[1])
+        for k, m in enumerate(tuning.get("bucket_mult", [])[: MAX_K + 1]):
+            t.bucket_mult[k] = int(m)
+        _check(self._lib.gst_engine_set_tuning(self._h, ctypes.byref(t)), "set_tuning")
 
     def server(self) -> "Server":
         return Server(self)

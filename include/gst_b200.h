@@ -132,6 +132,24 @@ typedef struct {
 gst_status gst_engine_create(const gst_engine_config* cfg, gst_engine** out);
 void gst_engine_destroy(gst_engine* e);
 
+/* Launch and scheduling parameters of an engine.  The defaults were picked
+ * by hand; gst_b200.autotune (Python) times candidates on a workload and
+ * writes a parameter file that sets them.  A field left 0 keeps the current
+ * value.  No reference counterpart (the reference fixes its launch shapes as
+ * macros: code/TrimCDP-WB/include/util.h:19-33, header.h:14). */
+typedef struct {
+  int grow_lanes;      /* lanes relaxing one grow chunk: 8, 16 or 32 (default 16) */
+  int rounds_per_poll; /* device rounds between host status checks (default 8) */
+  int max_slots;       /* queries resident at once, 1..1024 */
+  int chunk_pairs[GST_MAX_K + 1][2]; /* (edge, set) pairs per grow chunk by k and
+                                        [0] plain / [1] diameter-bounded (default 1024) */
+  int bucket_mult[GST_MAX_K + 1];    /* plain grows: cost-bucket width = this many times
+                                        the typical lightest edge, by k (default 1) */
+} gst_tuning;
+
+gst_status gst_engine_set_tuning(gst_engine* e, const gst_tuning* t);
+gst_status gst_engine_get_tuning(gst_engine* e, gst_tuning* out);
+
 /* Uploads the graph (CSR as gst_csr describes) and checks it: ids in range,
  * weights in [0, 2^30).  Replaces the per-program CSR upload
  * (csr_graph.hpp:117-125; code/TrimCDP-WB/include/gpu_graph.cuh:10-57). */
