@@ -44,6 +44,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "gpu4gst-1_b200"))
 sys.path.insert(0, ROOT)
 
+from gst_b200.clocks import ClockSampler  # noqa: E402
+
 METRIC = "GST queries/sec (k=3/5/7) batched vs 1-query GPU at exact cost; p50/p99; HBM %"
 
 WORKLOADS = {
@@ -167,59 +169,6 @@ def random_read_ceiling(torch, device) -> dict:
     torch.cuda.empty_cache()
     return {"reads_per_s": (64 << 20) / (best / 1e3), "sector_gbs": (64 << 20) * 32 / (best / 1e3) / 1e9,
             "how": "torch.take: 64 Mi random int32 reads from a 4 GiB array, best of 4"}
-
-
-class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
-
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-
-    def __init__(self, device: int):
-        self.device = device
-        self.proc = None
-        self.lines = []
-
-    def start(self):
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except OSError:
-            self.proc = None
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            p = [x.strip() for x in ln.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1]))
-                mx = float(p[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, p[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
 
 
 def flush_l2(torch, buf):
@@ -517,6 +466,8 @@ def main():
     ap.add_argument("--serve-queries", type=int, default=10000, help="c5: queries per rate")
     ap.add_argument("--ref-budget", type=float, default=150.0,
                     help="reference arm: seconds each reference process runs after its first query")
+    ap.add_argument("--tuning", default="auto",
+                    help="engine parameter file (auto: gpu4gst-1_b200/tuning/<workload>.json if present; none)")
     ap.add_argument("--write-dataset", default="", help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.write_dataset:
@@ -554,6 +505,17 @@ def main():
                           bucket_shift=args.bucket_shift)
     eng.load_graph(wl.graph.rowptr, wl.graph.col, wl.graph.w)
     eng.load_groups(wl.groups.ptr, wl.groups.mem)
+    tuning_file = None
+    if args.tuning != "none":
+        tuning_file = (os.path.join(ROOT, "gpu4gst-1_b200", "tuning", f"{args.workload}.json")
+                       if args.tuning == "auto" else args.tuning)
+        if os.path.exists(tuning_file):
+            eng.load_tuning(tuning_file)
+        else:
+            tuning_file = None
+    for key, v in (("rounds_per_poll", args.rounds_per_poll), ("max_slots", args.max_slots)):
+        if v:  # explicit flags win over the parameter file
+            eng.set_tuning({key: v})
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
     for _ in range(args.warmup):
@@ -644,7 +606,10 @@ def main():
                    **({"query_filter": f"k={args.k or 'any'} kind={args.kind} first={args.queries or 'all'}"}
                       if not unfiltered else {}),
                    "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before every step; "
-                   "per-query DP tables (GBs per step) exceed L2"},
+                   "per-query DP tables (GBs per step) exceed L2",
+                   "tuning": {"file": os.path.relpath(tuning_file, ROOT) if tuning_file else None,
+                              "params": {k: v for k, v in eng.get_tuning().items()
+                                         if k in ("grow_lanes", "rounds_per_poll", "max_slots")}}},
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "gpu_launches": launches,

@@ -337,6 +337,14 @@ class Engine:
             t.bucket_mult[k] = int(m)
         _check(self._lib.gst_engine_set_tuning(self._h, ctypes.byref(t)), "set_tuning")
 
+    def load_tuning(self, path: str) -> dict:
+        """Applies a parameter file written by gst_b200.autotune; returns the
+        tuning it set."""
+        from .autotune import load
+        t = load(path)
+        self.set_tuning(t)
+        return t
+
     def server(self) -> "Server":
         return Server(self)
 
