@@ -934,9 +934,12 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
 // reach it), kept out of line so the relaxation loop stays small.
 // dist: a per-thread scratch of k ints (shared memory: the bound indexes it
 // by set bit, which would put a register array in local memory).
+// The bound reads the distances of the groups outside S only, so only those
+// are loaded.
 __device__ __forceinline__ bool lb_prunes(const int32_t* trow, int k, int W, int L, int S, int R1,
                                           const int32_t* lbtab, int nc, int best, int* dist) {
-  for (int i = 0; i < k; ++i) {
+  for (int x = (W - 1) ^ S; x; x &= x - 1) {
+    const int i = __ffs(x) - 1;
     int dm = INF;
     for (int l = 0; l < L; ++l) dm = imin(dm, trow[(1 + i) * L + l]);
     dist[i] = clip_dist(dm, R1);
@@ -1004,7 +1007,9 @@ __device__ __forceinline__ int grow_improve(Slot& q, long long V, uint32_t u, in
   const bool pruned = s >= 2 && lb_prunes(trow, k, W, L, rS >> 8, q.R1, q.lbtab, nc, best, dist);
   const int old = atomicMin(&trow[tidx + td], nc);
   if (old <= nc) return 0;
-  touch(q, u);
+  // a vertex with a finite entry is on the touched list already (whoever set
+  // the entry touched it), so only a first finite entry needs the flag read
+  if (old >= INF) touch(q, u);
   if (pruned) return 0;
   if (s == 1 && (!hop || td <= (D + 1) / 2)) star_bound(q, trow, k, L, hop ? D / 2 : 0, hop ? (D + 1) / 2 : 0);
   if (2LL * nc <= best) {
