@@ -773,6 +773,8 @@ class Engine {
       res.stats.relax = (int64_t)q.st_relax;
       res.stats.improve = (int64_t)q.st_improve;
       res.stats.merges = (int64_t)q.st_merges;
+      res.stats.merge_items = (int64_t)q.st_mitems;
+      res.stats.merge_passed = (int64_t)q.st_mpassed;
       res.stats.touched = q.ntouched;
       if (q.phase == PH_ERROR || q.err != ERR_NONE) {
         static const char* why[] = {"", "chunk list overflow", "frontier list overflow",

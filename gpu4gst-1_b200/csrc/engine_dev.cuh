@@ -122,6 +122,7 @@ struct Slot {
   int32_t use_dead;
   unsigned long long answer;  // (cost << 32) | root
   unsigned long long st_frontier, st_relax, st_improve, st_merges;
+  unsigned long long st_mitems, st_mpassed;  // merge items visited / past the pre-filter
 };
 
 struct SlotStatus {

@@ -589,6 +589,15 @@ __device__ __forceinline__ void merge_costs(const int32_t* row, const uint8_t* s
   }
 }
 
+// Adds a run of merge statistics to slot t (nothing for t < 0).
+__device__ __forceinline__ void flush_merge_counts(Slot* slots, int t, unsigned long long items,
+                                                   unsigned long long passed, unsigned long long splits) {
+  if (t < 0) return;
+  if (items) atomicAdd(&slots[t].st_mitems, items);
+  if (passed) atomicAdd(&slots[t].st_mpassed, passed);
+  if (splits) atomicAdd(&slots[t].st_merges, splits);
+}
+
 // Returns whether the split loop ran (false: the lower-bound pre-filter
 // rejected the item).  vdist: the vertex's clipped singleton distances and
 // vmiss: the groups with no singleton entry at the vertex, both computed
@@ -690,6 +699,8 @@ k_merge_t(Slot* slots, const Plan* plan, Graph g) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   // every lane of a warp iterates the same number of times (shuffles below)
   const long long span = (total + 31) & ~31ll;
+  int acc_slot = -1;  // warp-uniform statistics run (see the loop's end)
+  unsigned long long acc_items = 0, acc_passed = 0, acc_splits = 0;
   for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < span; gi += stride) {
     unsigned long long ans = ~0ull, dirty = 0, key = ~0ull;
     int dmin = INF;
@@ -794,16 +805,29 @@ k_merge_t(Slot* slots, const Plan* plan, Graph g) {
         if ((int)dm < *(volatile int*)&q.next_min) atomicMin(&q.next_min, (int)dm);
       }
     }
-    // split counter (statistics): a plain warp sum when the warp is one slot
+    // statistics (items visited, items past the pre-filter, splits): warp
+    // sums accumulated while the warp stays on one slot and flushed when it
+    // changes (one atomic per counter and run instead of per iteration); a
+    // warp spanning slots adds each slot's segment directly
     {
       const int tf = __shfl_sync(0xffffffffu, t, 0), tl = __shfl_sync(0xffffffffu, t, 31);
+      const unsigned long long packed =
+          t >= 0 ? (1ull | (nsplit ? 1ull << 8 : 0ull) | ((unsigned long long)nsplit << 16)) : 0ull;
       if (tf == tl && tf >= 0) {
-        const unsigned ns = __reduce_add_sync(0xffffffffu, (unsigned)nsplit);
-        if ((threadIdx.x & 31) == 0 && ns) atomicAdd(&slots[tf].st_merges, (unsigned long long)ns);
+        unsigned long long sum = packed;
+        for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (tf != acc_slot) {
+          if (lane == 0) flush_merge_counts(slots, acc_slot, acc_items, acc_passed, acc_splits);
+          acc_slot = tf;
+          acc_items = acc_passed = acc_splits = 0;
+        }
+        acc_items += sum & 0xff;
+        acc_passed += (sum >> 8) & 0xff;
+        acc_splits += sum >> 16;
       } else {
-        const unsigned long long ns = seg_add_u64(nsplit, skey);
+        const unsigned long long sum = seg_add_u64(packed, skey);
         const bool shead = seg_head(skey);  // every lane: a full-warp shuffle
-        if (t >= 0 && shead && ns) atomicAdd(&slots[t].st_merges, ns);
+        if (t >= 0 && shead) flush_merge_counts(slots, t, sum & 0xff, (sum >> 8) & 0xff, sum >> 16);
       }
     }
     // live-list append: one vertex per nS items appends, so most warps skip
@@ -824,6 +848,7 @@ k_merge_t(Slot* slots, const Plan* plan, Graph g) {
       }
     }
   }
+  if (lane == 0) flush_merge_counts(slots, acc_slot, acc_items, acc_passed, acc_splits);
 }
 
 // ---------------------------------------------------------------------------

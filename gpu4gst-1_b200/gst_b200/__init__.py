@@ -81,7 +81,8 @@ class _Tuning(ctypes.Structure):
 
 class _Stats(ctypes.Structure):
     _fields_ = [("rounds", ctypes.c_int64), ("frontier", ctypes.c_int64), ("relax", ctypes.c_int64),
-                ("improve", ctypes.c_int64), ("merges", ctypes.c_int64), ("touched", ctypes.c_int64),
+                ("improve", ctypes.c_int64), ("merges", ctypes.c_int64), ("merge_items", ctypes.c_int64),
+                ("merge_passed", ctypes.c_int64), ("touched", ctypes.c_int64),
                 ("device_ms", ctypes.c_double), ("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
 
 

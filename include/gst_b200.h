@@ -166,6 +166,8 @@ typedef struct {
   int64_t relax;        /* edge relaxations attempted */
   int64_t improve;      /* successful table updates (grow) */
   int64_t merges;       /* merge partner pairs evaluated (past the lower-bound pre-filter) */
+  int64_t merge_items;  /* (vertex, set) items the merges visited */
+  int64_t merge_passed; /* of those, items past the lower-bound pre-filter */
   int64_t touched;      /* vertices that held a finite state */
   double device_ms;     /* device time from admission to answer */
   double queue_ms;      /* host time from submission to admission into a slot */
