@@ -334,8 +334,18 @@ class Engine {
     }
     std::memset(&prof_, 0, sizeof prof_);
     GST_CUDA(cudaEventRecord(ev_run0_, stream_));
+    // largest tables first (longest-processing-time order): the queries that
+    // hold the most memory start early and the small ones fill the gaps,
+    // instead of a large query starting last and running alone at the end
+    std::vector<std::pair<size_t, std::shared_ptr<Request>>> order;
     for (auto& r : reqs)
-      if (r && !r->done) pending_.push_back(r);
+      if (r && !r->done) {
+        const Shape sh{(int)r->groups.size(), r->D < 0 ? 1 : r->D + 1};
+        order.emplace_back(slab_bytes(sh, nullptr), r);
+      }
+    std::stable_sort(order.begin(), order.end(),
+                     [](const auto& a, const auto& b) { return a.first > b.first; });
+    for (auto& o : order) pending_.push_back(o.second);
     while (true) {
       gst_status s = step();
       if (s != GST_OK) return s;
@@ -496,7 +506,7 @@ class Engine {
   }
 
   // A clean slab of the shape: cached, or carved and initialised.
-  bool acquire_slab(Shape sh, Slab* out) {
+  bool acquire_slab(Shape sh, Slab* out, bool evict = true) {
     auto it = cache_.find(sh);
     if (it != cache_.end() && !it->second.empty()) {
       *out = it->second.back();
@@ -507,6 +517,7 @@ class Engine {
     size_t bytes = slab_bytes(sh, &s);
     size_t off = arena_alloc_.alloc(bytes);
     if (off == SIZE_MAX) {  // evict cached slabs of other shapes and retry
+      if (!evict) return false;
       clear_slab_cache();
       off = arena_alloc_.alloc(bytes);
       if (off == SIZE_MAX) return false;
@@ -560,26 +571,36 @@ class Engine {
     }
   }
 
+  // Admits pending queries into free slots while their slabs fit.  When the
+  // first pending query does not fit yet, later ones that fit are admitted
+  // past it (the memory it waits for is not freed any sooner by idling),
+  // but at most kMaxBypass times in a row, so it cannot starve.
+  static constexpr int kMaxBypass = 256;
   gst_status admit() {
-    while (!pending_.empty()) {
+    size_t pi = 0;
+    while (pi < pending_.size()) {
       int t = -1;
       for (int i = 0; i < max_slots_; ++i)
         if (!slot_busy_[i]) { t = i; break; }
       if (t < 0) break;
-      auto r = pending_.front();
+      auto r = pending_[pi];
       const int k = (int)r->groups.size();
       Shape sh{k, r->D < 0 ? 1 : r->D + 1};
       Slab sb;
-      if (!acquire_slab(sh, &sb)) {
-        if (active_ == 0) {  // cannot fit even alone
+      if (!acquire_slab(sh, &sb, /*evict=*/pi == 0)) {
+        if (pi == 0 && active_ == 0) {  // cannot fit even alone
           pending_.pop_front();
           r->status = fail(GST_E_NOMEM, "query needs more than the device arena");
           r->done = true;
           continue;
         }
-        break;  // wait for running queries to free memory
+        if (pi == 0 && bypassed_ >= kMaxBypass) break;  // let the front one have the memory
+        ++pi;
+        continue;
       }
-      pending_.pop_front();
+      pending_.erase(pending_.begin() + (std::ptrdiff_t)pi);
+      bypassed_ = pi == 0 ? 0 : bypassed_ + 1;
+      pi = 0;
       r->t_admit = std::chrono::steady_clock::now();
       Slot& q = h_slot_[t];  // its previous copy finished: the slot was harvested after a sync
       std::memset(&q, 0, sizeof q);
@@ -878,6 +899,7 @@ class Engine {
   std::vector<std::shared_ptr<Request>> slot_req_;
   std::vector<Slab> slot_slab_;
   int nslots_hw_ = 0;
+  int bypassed_ = 0;  // admissions past a pending front query that did not fit
   cudaGraphExec_t graph_exec_ = nullptr;
   int graph_rounds_ = 0, graph_slots_ = 0;
   bool profile_ = false;
