@@ -215,15 +215,17 @@ def _write_dataset_main(name: str, out_dir: str) -> None:
 
 def run_ref_timed(exe: str, d: str, name: str, k: int, a: int, b: int, budget_s: float):
     """Runs the reference PrunedDP++ on queries a..b of <name><k>.csv and
-    times each query from its own progress lines ("<data> iteration i" is
-    printed when query i starts; the process ends after the last one), so
-    the graph load is excluded and each query's own preprocessing counted.
-    The process is stopped budget_s seconds after its first query started;
-    only the queries it finished are returned."""
+    times each query from its own progress lines: "<data> iteration i" is
+    printed when query i starts and a line of dashes when its solve and
+    feasibility check are done (code/PrunedDP++/include/exp_CPU_nonHop.h:90-127),
+    so the graph load and the process's teardown are excluded and each
+    query's own preprocessing is counted.  The process is stopped budget_s
+    seconds after its first query started; only the queries it finished are
+    returned."""
     p = subprocess.Popen([exe, "1", d + "/", name, str(k), str(a), str(b)], stdout=subprocess.PIPE,
                          stderr=subprocess.DEVNULL, stdin=subprocess.DEVNULL, text=True)
-    starts = []
-    ended = []
+    times = []
+    t_start = None
     timer = None
 
     def stop():
@@ -232,17 +234,17 @@ def run_ref_timed(exe: str, d: str, name: str, k: int, a: int, b: int, budget_s:
 
     for line in p.stdout:
         if " iteration " in line:
-            starts.append(time.perf_counter())
+            t_start = time.perf_counter()
             if timer is None:
                 timer = threading.Timer(budget_s, stop)
                 timer.start()
-        elif "END" in line and "runningtime" in line:
-            ended.append(time.perf_counter())
+        elif line.startswith("-----") and t_start is not None:
+            times.append(time.perf_counter() - t_start)
+            t_start = None
     p.wait()
     if timer is not None:
         timer.cancel()
-    bounds = starts[1:] + ended[:1]
-    return [t1 - t0 for t0, t1 in zip(starts, bounds)]
+    return times
 
 
 def cpu_reference_sample(name: str, per_k: int, budget_s: float = 600):
