@@ -220,8 +220,9 @@ def run_ref_timed(exe: str, d: str, name: str, k: int, a: int, b: int, budget_s:
     feasibility check are done (code/PrunedDP++/include/exp_CPU_nonHop.h:90-127),
     so the graph load and the process's teardown are excluded and each
     query's own preprocessing is counted.  The process is stopped budget_s
-    seconds after its first query started; only the queries it finished are
-    returned."""
+    seconds after its first query started.  Returns (the finished queries'
+    times, the time the unfinished query had run when it was stopped, or
+    None): the latter is a lower bound on that query's time."""
     p = subprocess.Popen([exe, "1", d + "/", name, str(k), str(a), str(b)], stdout=subprocess.PIPE,
                          stderr=subprocess.DEVNULL, stdin=subprocess.DEVNULL, text=True)
     times = []
@@ -244,13 +245,16 @@ def run_ref_timed(exe: str, d: str, name: str, k: int, a: int, b: int, budget_s:
     p.wait()
     if timer is not None:
         timer.cancel()
-    return times
+    cut = time.perf_counter() - t_start if t_start is not None else None
+    return times, cut
 
 
-def cpu_reference_sample(name: str, per_k: int, budget_s: float = 600):
+def cpu_reference_sample(name: str, per_k: int, budget_s: float = 300):
     """The reference PrunedDP++ (oracle/_ref) on the first per_k plain
     queries of each k of the workload, one single-threaded process per query,
-    all at once.  Returns per-class mean seconds per query and what ran."""
+    all at once, each stopped budget_s seconds after its query started.
+    Returns per-class mean seconds per query (a stopped query counts with the
+    time it had run: a lower bound) and what ran."""
     import oracle
     exe = oracle.ref_binary("PrunedDP++")
     if not os.path.exists(exe):
@@ -270,12 +274,15 @@ def cpu_reference_sample(name: str, per_k: int, budget_s: float = 600):
         t.start()
     for t in ths:
         t.join()
-    per = {}
-    for (k, i), ts in zip(jobs, out):
+    per, stopped = {}, 0
+    for (k, i), (ts, cut) in zip(jobs, out):
         if ts:
             per.setdefault(k, []).append(ts[0])
+        elif cut is not None:
+            per.setdefault(k, []).append(cut)
+            stopped += 1
     return {"per_k_s": {k: statistics.mean(v) for k, v in per.items()}, "queries": len(jobs),
-            "per_k": per_k}
+            "per_k": per_k, "stopped": stopped, "budget_s": budget_s}
 
 
 def cpu_mix_qps(per_k_s: dict, queries, cores: int):
@@ -419,19 +426,24 @@ def run_reference_arm(args):
         t.start()
     for t in ths:
         t.join()
-    per_k = {}
-    for k, ts in got.values():
-        timed = ts[args.warmup:] if len(ts) > args.warmup else ts
-        per_k.setdefault(k, []).extend(timed)
+    # the graph load of each process is its warm-up; a query still running at
+    # the budget counts with the time it had run (a lower bound on its time)
+    per_k, stopped = {}, 0
+    for k, (ts, cut) in got.values():
+        per_k.setdefault(k, []).extend(ts)
+        if not ts and cut is not None:
+            per_k[k].append(cut)
+            stopped += 1
     mean_k = {k: statistics.mean(v) for k, v in per_k.items() if v}
     weights = {k: len(v) for k, v in byk.items() if k in mean_k}
     t_mix = sum(weights[k] * mean_k[k] for k in weights) / sum(weights.values())
     v = procs / t_mix
     nq = sum(len(v) for v in per_k.values())
     sample = (f"{nq} timed plain queries of the {args.workload.upper()} workload on {procs} single-threaded "
-              f"PrunedDP++ processes (k per process cycling over {ks}, {args.warmup} warm-up queries each, "
-              f"stopped {args.ref_budget:.0f} s after the first query); per-query time from the reference's "
-              f"progress lines (graph load excluded); mean s per query by k: "
+              f"PrunedDP++ processes (process p runs k = {ks}[p mod {len(ks)}], stopped {args.ref_budget:.0f} s "
+              f"after its first query; {stopped} stopped in their first query count with the time they had "
+              f"run); per-query time from the reference's progress lines (graph load excluded); "
+              f"value = {procs} / the plain-query mix's mean s per query; mean s by k: "
               + ", ".join(f"k={k}: {mean_k[k]:.2f}" for k in sorted(mean_k)))
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": args.gpus,
@@ -466,8 +478,11 @@ def main():
                     help="also run the reference GPU TrimCDP on this many plain queries (comparator)")
     ap.add_argument("--rates", default="50,200,1000", help="c5: Poisson arrival rates, queries/s")
     ap.add_argument("--serve-queries", type=int, default=10000, help="c5: queries per rate")
-    ap.add_argument("--ref-budget", type=float, default=150.0,
+    ap.add_argument("--ref-budget", type=float, default=360.0,
                     help="reference arm: seconds each reference process runs after its first query")
+    ap.add_argument("--cpu-per-k", type=int, default=1, help="cpu_baseline: plain queries per k")
+    ap.add_argument("--cpu-budget", type=float, default=300.0,
+                    help="cpu_baseline: seconds a reference process may run its query")
     ap.add_argument("--tuning", default="auto",
                     help="engine parameter file (auto: gpu4gst-1_b200/tuning/<workload>.json if present; none)")
     ap.add_argument("--write-dataset", default="", help=argparse.SUPPRESS)
@@ -496,8 +511,16 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
 
-    wl = make_workload(args.workload, rank)
     unfiltered = not (args.k or args.kind != "all" or args.queries)
+    # the reference CPU sample runs on host cores while the GPU steps run
+    cpu_sample = {}
+    cpu_thread = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and unfiltered:
+        def _cpu():
+            cpu_sample["r"] = cpu_reference_sample(args.workload, per_k=args.cpu_per_k, budget_s=args.cpu_budget)
+        cpu_thread = threading.Thread(target=_cpu, daemon=True)
+        cpu_thread.start()
+    wl = make_workload(args.workload, rank)
     filter_queries(wl, args)
     queries = [q for q, _ in wl.queries]
     Ds = [D for _, D in wl.queries]
@@ -640,16 +663,19 @@ def main():
                                       "frac": grow_reads / ceiling["reads_per_s"] if grow_reads else None}},
         "clocks": clocks,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and unfiltered:
+    if cpu_thread is not None:
+        cpu_thread.join()
         cores = max(1, min(os.cpu_count() or 1, 32))
-        smp = cpu_reference_sample(args.workload, per_k=2)
+        smp = cpu_sample.get("r")
         if smp is not None:
             qps = cpu_mix_qps(smp["per_k_s"], wl.queries, cores)
             out["cpu_baseline"] = {
                 "value": qps, "unit": "queries/s", "cores": cores, "kind": "reference",
                 "sample": f"the first {smp['per_k']} plain queries of each k of this workload, one "
-                          f"single-threaded PrunedDP++ process each ({smp['queries']} at once); per-query "
-                          f"time from the reference's progress lines (graph load excluded); value = "
+                          f"single-threaded PrunedDP++ process each ({smp['queries']} at once, on host cores "
+                          f"while the GPU steps ran); per-query time from the reference's progress lines "
+                          f"(graph load excluded); {smp['stopped']} queries still running after "
+                          f"{smp['budget_s']:.0f} s count with the time they had run (a lower bound); value = "
                           f"{cores} cores / the plain-query mix's mean time per query; mean s per query "
                           "by k: " + ", ".join(f"k={k}: {t:.2f}" for k, t in sorted(smp["per_k_s"].items()))}
     if rank == 0 and args.ref_gpu > 0:
