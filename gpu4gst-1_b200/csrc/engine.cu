@@ -103,6 +103,7 @@ struct Slab {
   uint32_t* touched = nullptr;
   uint32_t* tflag = nullptr;
   uint32_t* dead = nullptr;
+  int32_t* sd = nullptr;
   Chunk* chunks = nullptr;
   int32_t* lbtab = nullptr;
   int32_t* wstack = nullptr;
@@ -453,6 +454,7 @@ class Engine {
     size_t o_touched = take(V * 4);
     size_t o_tflag = take(V * 4);
     size_t o_dead = take((V + 31) / 32 * 4);
+    size_t o_sd = take(V * 32);
     size_t o_chunks = take((size_t)s.chunk_cap * sizeof(Chunk));
     size_t o_lbtab = take((size_t)sh.k * sh.k * W * 4 + (size_t)sh.k * W * 4);
     size_t o_wstack = take((size_t)s.wcap * 16);
@@ -467,6 +469,7 @@ class Engine {
       out->touched = reinterpret_cast<uint32_t*>(o_touched);
       out->tflag = reinterpret_cast<uint32_t*>(o_tflag);
       out->dead = reinterpret_cast<uint32_t*>(o_dead);
+      out->sd = reinterpret_cast<int32_t*>(o_sd);
       out->chunks = reinterpret_cast<Chunk*>(o_chunks);
       out->lbtab = reinterpret_cast<int32_t*>(o_lbtab);
       out->wstack = reinterpret_cast<int32_t*>(o_wstack);
@@ -530,6 +533,7 @@ class Engine {
     place(s.touched);
     place(s.tflag);
     place(s.dead);
+    place(s.sd);
     place(s.chunks);
     place(s.lbtab);
     place(s.wstack);
@@ -540,7 +544,8 @@ class Engine {
     if (cudaMemsetAsync(s.table, 0x3f, V * W * L * 4, stream_) != cudaSuccess ||
         cudaMemsetAsync(s.mask, 0, (sh.L == 1 ? 2 : L) * V * 8, stream_) != cudaSuccess ||
         cudaMemsetAsync(s.tflag, 0, V * 4, stream_) != cudaSuccess ||
-        cudaMemsetAsync(s.dead, 0, (V + 31) / 32 * 4, stream_) != cudaSuccess) {
+        cudaMemsetAsync(s.dead, 0, (V + 31) / 32 * 4, stream_) != cudaSuccess ||
+        cudaMemsetAsync(s.sd, 0x3f, V * 32, stream_) != cudaSuccess) {
       arena_alloc_.release(off, bytes);
       return false;
     }
@@ -610,6 +615,7 @@ class Engine {
       q.touched = sb.touched;
       q.tflag = sb.tflag;
       q.dead = sb.dead;
+      q.sd = sb.sd;
       q.chunks = sb.chunks;
       q.lbtab = sb.lbtab;
       q.wstack = sb.wstack;
@@ -844,6 +850,7 @@ class Engine {
         GST_CUDA(cudaMemsetAsync(sb.mask, 0, (L == 1 ? 2 : L) * V * 8, stream_));
         GST_CUDA(cudaMemsetAsync(sb.tflag, 0, V * 4, stream_));
         GST_CUDA(cudaMemsetAsync(sb.dead, 0, (V + 31) / 32 * 4, stream_));
+        GST_CUDA(cudaMemsetAsync(sb.sd, 0x3f, V * 32, stream_));
       }
       k_free_slot<<<1, 1, 0, stream_>>>(d_slots_, t);
       GST_CUDA(cudaGetLastError());

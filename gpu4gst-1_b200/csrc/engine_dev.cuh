@@ -17,6 +17,8 @@
 //                          lists 2/3, ping-pong; D-: one list per depth label).
 //   touched[], tflag[v]   vertices that ever held a finite entry.
 //   dead[V / 32]          vertices the liveness test dropped (bitmap).
+//   sd[v][8]              v's singleton minima over labels, one sector per
+//                          vertex, filled by the first merge.
 //   live[2][V]            merge lists: the vertices a layer's merge visits;
 //                          each merge writes, for the next layer, the vertices
 //                          whose whole-tree lower bound is still <= best
@@ -120,6 +122,11 @@ struct Slot {
   // queries); grows and preps skip such vertices while use_dead is set
   uint32_t* dead;
   int32_t use_dead;
+  // sd[v * 8 + i]: min over depth labels of v's singleton entry of group i
+  // (INF: none), written by the query's first merge, when layer 1 is final;
+  // later merges and the grow's lower bound read it instead of the row
+  int32_t* sd;
+  int32_t sd_ready;
   unsigned long long answer;  // (cost << 32) | root
   unsigned long long st_frontier, st_relax, st_improve, st_merges;
   unsigned long long st_mitems, st_mpassed;  // merge items visited / past the pre-filter

@@ -247,7 +247,7 @@ __global__ void k_ctl_a(Slot* slots, int nslots, Plan* plan, SlotStatus* status)
               q.d += 1;
             }
             break;
-          case A_MERGE: if (hop) q.d = 0; break;
+          case A_MERGE: if (hop) q.d = 0; q.sd_ready = 1; break;
           case A_MERGEFULL: q.phase = PH_DONE; done = true; break;
           default: break;
         }
@@ -737,14 +737,28 @@ k_merge_t(Slot* slots, const Plan* plan, Graph g) {
     if (t >= 0) {
       const Slot& q = slots[t];
       const int k = q.k, L = q.L, R1 = q.R1;
-      const int32_t* row = q.table + (long long)v * ((long long)q.W * L);
       const int off = __popc(seg & ((1u << lane) - 1)), seglen = __popc(seg);
+      int32_t* sdv = q.sd + (long long)v * 8;
       unsigned mm = 0;
-      for (int i = off; i < k; i += seglen) {
-        int dm = INF;
-        for (int l = 0; l < L; ++l) dm = imin(dm, row[(1 + i) * L + l]);
-        s_vdist[(wbase + head) * DIST_STRIDE + i] = clip_dist(dm, R1);
-        if (dm >= INF) mm |= 1u << i;
+      // D-queries read the minima from sd once it is filled (one sector
+      // instead of k * L row entries); plain rows hold one label, whose
+      // singleton entries share a sector the split loop reads anyway
+      if (q.sd_ready && L > 1) {
+        for (int i = off; i < k; i += seglen) {
+          const int dm = sdv[i];
+          s_vdist[(wbase + head) * DIST_STRIDE + i] = clip_dist(dm, R1);
+          if (dm >= INF) mm |= 1u << i;
+        }
+      } else {
+        const int32_t* row = q.table + (long long)v * ((long long)q.W * L);
+        const bool first = !q.sd_ready;  // the query's first merge: layer 1 is final, keep its minima
+        for (int i = off; i < k; i += seglen) {
+          int dm = INF;
+          for (int l = 0; l < L; ++l) dm = imin(dm, row[(1 + i) * L + l]);
+          if (first) sdv[i] = dm;
+          s_vdist[(wbase + head) * DIST_STRIDE + i] = clip_dist(dm, R1);
+          if (dm >= INF) mm |= 1u << i;
+        }
       }
       if (mm) atomicOr(&s_vmiss[wbase + head], mm);
     }
@@ -961,13 +975,13 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
 // by set bit, which would put a register array in local memory).
 // The bound reads the distances of the groups outside S only, so only those
 // are loaded.
-__device__ __forceinline__ bool lb_prunes(const int32_t* trow, int k, int W, int L, int S, int R1,
+// Layers >= 2 only: the singleton minima come from sd (one sector) rather
+// than from the target row.
+__device__ __forceinline__ bool lb_prunes(const int32_t* sdu, int k, int W, int S, int R1,
                                           const int32_t* lbtab, int nc, int best, int* dist) {
   for (int x = (W - 1) ^ S; x; x &= x - 1) {
     const int i = __ffs(x) - 1;
-    int dm = INF;
-    for (int l = 0; l < L; ++l) dm = imin(dm, trow[(1 + i) * L + l]);
-    dist[i] = clip_dist(dm, R1);
+    dist[i] = clip_dist(sdu[i], R1);
   }
   return (long long)nc + lower_bound(dist, k, W, S, lbtab, (long long)best - nc) > best;
 }
@@ -1026,20 +1040,23 @@ __device__ __forceinline__ int grow_improve(Slot& q, long long V, uint32_t u, in
   int32_t* trow = q.table + (long long)u * (W * L);
   const long long tidx = (long long)(c_sub.loff[k][s] + r) * L;
   // A candidate that fails the lower-bound test is still a real derivation
-  // cost: store it (unmarked, so never grown from) so that later, costlier
-  // candidates for this state stop at the plain read instead of re-running
-  // the bound.
-  const bool pruned = s >= 2 && lb_prunes(trow, k, W, L, rS >> 8, q.R1, q.lbtab, nc, best, dist);
+  // cost: it is stored (unmarked, so never grown from) so that later,
+  // costlier candidates for this state stop at the plain read instead of
+  // re-running the bound.  The bound only decides whether a stored candidate
+  // is grown from, so it is skipped when the candidate is not a grow source
+  // anyway (cost above best/2, or the last depth label).
+  const bool source = 2LL * nc <= best && (!hop || td < D);
+  const bool pruned = s >= 2 && source && lb_prunes(q.sd + (long long)u * 8, k, W, rS >> 8, q.R1, q.lbtab, nc, best, dist);
   const int old = atomicMin(&trow[tidx + td], nc);
   if (old <= nc) return 0;
   // a vertex with a finite entry is on the touched list already (whoever set
   // the entry touched it), so only a first finite entry needs the flag read
   if (old >= INF) touch(q, u);
-  if (pruned) return 0;
+  if (pruned) return 1;
   if (s == 1 && (!hop || td <= (D + 1) / 2)) star_bound(q, trow, k, L, hop ? D / 2 : 0, hop ? (D + 1) / 2 : 0);
-  if (2LL * nc <= best) {
+  if (source) {
     if (!hop) mark_plain(q, V, u, r, nc);
-    else if (td < D) mark_dirty(q, V, u, r, td, td);
+    else mark_dirty(q, V, u, r, td, td);
   }
   return 1;
 }
@@ -1067,6 +1084,7 @@ k_grow_t(Slot* slots, const Plan* plan, Graph g) {
   const long long total = s_off[ng];
   const long long nwarps = (long long)gridDim.x * GROW_WARPS;
   unsigned long long nrel = 0, nimp = 0;  // flushed when the slot changes
+  unsigned nrel32 = 0;  // this unit's relaxations (a 32-bit counter in the loop needs fewer registers)
   int cur_slot = -1;
   for (long long gi = blockIdx.x * (long long)GROW_WARPS + wib; gi < total; gi += nwarps) {
     const int j = seg_search(s_off, ng, gi);
@@ -1130,7 +1148,7 @@ k_grow_t(Slot* slots, const Plan* plan, Graph g) {
             a = __ldg(&g.adj[e]);
             rS = gr[bi];
             nc = gsv[bi] + a.y;
-            ++nrel;
+            ++nrel32;
             if (use_dead && ((q.dead[(uint32_t)a.x >> 5] >> (a.x & 31)) & 1u)) nc = INF;
           }
           e += qG;
@@ -1161,6 +1179,8 @@ k_grow_t(Slot* slots, const Plan* plan, Graph g) {
       }
     }
     __syncwarp();
+    nrel += nrel32;
+    nrel32 = 0;
   }
   if (cur_slot >= 0) flush_counts(slots[cur_slot], nrel, nimp);
 }
@@ -1488,6 +1508,7 @@ __global__ void k_reset(Slot* slots, int t, Graph g) {
     if (x % planes == 0) {
       q.tflag[v] = 0u;
       q.dead[v >> 5] = 0u;  // only touched vertices are ever marked
+      for (int i = 0; i < 8; ++i) q.sd[(long long)v * 8 + i] = INF;  // only touched vertices are ever written
     }
   }
 }

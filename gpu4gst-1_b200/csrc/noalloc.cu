@@ -218,6 +218,7 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   const size_t o_touched = take((size_t)V * 4);
   const size_t o_tflag = take((size_t)V * 4);
   const size_t o_dead = take(((size_t)V + 31) / 32 * 4);
+  const size_t o_sd = take((size_t)V * 32);
   const size_t o_chunks = take(chunk_cap * sizeof(Chunk));
   const size_t o_lbtab = take((size_t)kk * kk * W * 4 + (size_t)kk * W * 4);
   const size_t o_live = take(2 * (size_t)V * 4);
@@ -237,6 +238,7 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   q.touched = reinterpret_cast<uint32_t*>(base + o_touched);
   q.tflag = reinterpret_cast<uint32_t*>(base + o_tflag);
   q.dead = reinterpret_cast<uint32_t*>(base + o_dead);
+  q.sd = reinterpret_cast<int32_t*>(base + o_sd);
   q.chunks = reinterpret_cast<Chunk*>(base + o_chunks);
   q.lbtab = reinterpret_cast<int32_t*>(base + o_lbtab);
   q.live[0] = reinterpret_cast<uint32_t*>(base + o_live);
@@ -269,6 +271,7 @@ extern "C" gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_r
   if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_mask, 0, planes * (size_t)V * 8, s);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_tflag, 0, (size_t)V * 4, s);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_dead, 0, ((size_t)V + 31) / 32 * 4, s);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_sd, 0x3f, (size_t)V * 32, s);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(d_plan, 0, sizeof(Plan), s);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(base + o_acc, 0, 2 * sizeof(unsigned long long), s);
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_slot, &q, sizeof q, cudaMemcpyHostToDevice, s);

@@ -164,7 +164,7 @@ typedef struct {
   int64_t rounds;       /* device rounds the query took part in */
   int64_t frontier;     /* frontier states expanded (grow sources) */
   int64_t relax;        /* edge relaxations attempted */
-  int64_t improve;      /* successful table updates (grow) */
+  int64_t improve;      /* successful table updates by the grow */
   int64_t merges;       /* merge partner pairs evaluated (past the lower-bound pre-filter) */
   int64_t merge_items;  /* (vertex, set) items the merges visited */
   int64_t merge_passed; /* of those, items past the lower-bound pre-filter */
