@@ -119,36 +119,37 @@ __device__ __forceinline__ int lower_bound(const int* dist, int k, int W, int S,
   // Callers only ask whether the bound exceeds lim, so the parts are taken
   // cheapest first (one-label O(m), W2 tour O(m), pairwise tour O(m^2), m =
   // |X|) and the first that exceeds lim ends the evaluation; a bound <= lim
-  // is the exact maximum of the three.
+  // is the exact maximum of the three.  Unsigned 32-bit sums: every term is
+  // at most INF, and three of them stay below 2^32.
   const int Xs = (W - 1) ^ S;
   if (Xs == 0) return 0;
-  int one = 0, mind = INF;
+  unsigned one = 0, mind = INF;
   for (int x = Xs; x; x &= x - 1) {
-    const int d = dist[__ffs(x) - 1];
-    one = imax(one, d);
-    mind = imin(mind, d);
+    const unsigned d = (unsigned)dist[__ffs(x) - 1];
+    one = one > d ? one : d;
+    mind = mind < d ? mind : d;
   }
-  long long lb = one;
-  if (lb > lim) return (int)(lb < INF ? lb : INF);
+  unsigned lb = one;
+  if ((long long)lb > lim) return (int)(lb < INF ? lb : INF);
   const int32_t* W2 = lbtab + (size_t)k * k * W + Xs;
   for (int x = Xs; x; x &= x - 1) {
     const int i = __ffs(x) - 1;
-    const long long t2 = ((long long)dist[i] + W2[i * W] + mind + 1) >> 1;
+    const unsigned t2 = ((unsigned)dist[i] + (unsigned)W2[i * W] + mind + 1u) >> 1;
     if (t2 > lb) lb = t2;
   }
-  if (lb > lim) return (int)(lb < INF ? lb : INF);
-  long long t1 = 2LL * INF;
+  if ((long long)lb > lim) return (int)(lb < INF ? lb : INF);
+  unsigned t1 = 2u * INF;
   for (int x = Xs; x; x &= x - 1) {
     const int i = __ffs(x) - 1;
-    const long long di = dist[i];
+    const unsigned di = (unsigned)dist[i];
     const int32_t* Pi = lbtab + (size_t)i * k * W + Xs;
     for (int y = Xs; y; y &= y - 1) {
-      const int j = __ffs(y) - 1;
-      const long long t = di + Pi[j * W] + dist[j];
+      const int jj = __ffs(y) - 1;
+      const unsigned t = di + (unsigned)Pi[jj * W] + (unsigned)dist[jj];
       if (t < t1) t1 = t;
     }
   }
-  const long long lb1 = (t1 + 1) >> 1;
+  const unsigned lb1 = (t1 + 1u) >> 1;
   if (lb1 > lb && lb1 < INF) lb = lb1;
   return (int)(lb < INF ? lb : INF);
 }
@@ -565,13 +566,31 @@ __device__ __forceinline__ void merge_costs(const int32_t* row, const uint8_t* s
     } else {
       int a[LT > 0 ? LT : MAXL], b[LT > 0 ? LT : MAXL];
       int ma = INF, mb = INF;
+      if (LT > 1 && LT % 2 == 0) {
+        // an even label count keeps a set's labels 8-byte aligned: pairs per load
+        const int2* r1 = reinterpret_cast<const int2*>(row + i1);
+        const int2* r2 = reinterpret_cast<const int2*>(row + i2);
 #pragma unroll
-      for (int l = 0; l < (LT > 0 ? LT : MAXL); ++l) {
-        if (LT == 0 && l >= L) break;
-        ma = imin(ma, row[i1 + l]);
-        mb = imin(mb, row[i2 + l]);
-        a[l] = ma;
-        b[l] = mb;
+        for (int h = 0; h < (LT > 1 ? LT / 2 : 1); ++h) {
+          const int2 x = r1[h], y = r2[h];
+          ma = imin(ma, x.x);
+          mb = imin(mb, y.x);
+          a[2 * h] = ma;
+          b[2 * h] = mb;
+          ma = imin(ma, x.y);
+          mb = imin(mb, y.y);
+          a[2 * h + 1] = ma;
+          b[2 * h + 1] = mb;
+        }
+      } else {
+#pragma unroll
+        for (int l = 0; l < (LT > 0 ? LT : MAXL); ++l) {
+          if (LT == 0 && l >= L) break;
+          ma = imin(ma, row[i1 + l]);
+          mb = imin(mb, row[i2 + l]);
+          a[l] = ma;
+          b[l] = mb;
+        }
       }
 #pragma unroll
       for (int l = 0; l < (LT > 0 ? LT : MAXL); ++l) {
@@ -717,8 +736,15 @@ k_merge_t(Slot* slots, const Plan* plan, Graph g) {
         const int k = q.k, s = q.s;
         const int nS = c_sub.loff[k][s + 1] - c_sub.loff[k][s];
         const long long local = gi - s_off[j];
-        const int vi = (int)(local / nS);
-        r = (int)(local % nS);
+        int vi;
+        if (local < (1ll << 32)) {  // 32-bit division unless a slot holds 2^32 items
+          const unsigned l32 = (unsigned)local, q32 = l32 / (unsigned)nS;
+          vi = (int)q32;
+          r = (int)(l32 - q32 * (unsigned)nS);
+        } else {
+          vi = (int)(local / nS);
+          r = (int)(local % nS);
+        }
         v = vi < q.nlr ? q.live[q.lr][vi] : q.touched[q.mt0 + vi - q.nlr];
         key = ((unsigned long long)(unsigned)t << 32) | (unsigned)vi;
       } else {
