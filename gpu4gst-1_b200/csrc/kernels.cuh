@@ -991,8 +991,10 @@ __global__ void k_prep(Slot* slots, const Plan* plan, Graph g) {
 // Grow: one group of GROW_LANES lanes per chunk, 32 / GROW_LANES chunks of
 // one slot per warp.  Lanes walk (edge, dirty set) pairs with the set index
 // fastest, so the lanes relaxing one neighbour touch adjacent words of its
-// row.  A target is read before the atomicMin and the lower bound is only
-// evaluated for candidates that improve it.
+// row.  Each lane relaxes two pairs per step, so two independent
+// adjacency-then-target read chains are in flight per lane.  A target is read
+// before the atomicMin; candidates that beat it are queued per warp in shared
+// memory and handled in batches by grow_cold.
 // ---------------------------------------------------------------------------
 
 // Lower-bound test of a grow candidate (cold path: only improving candidates
@@ -1054,37 +1056,92 @@ __device__ __forceinline__ void star_bound(Slot& q, const int32_t* trow, int k, 
   if (ub < *(volatile int*)&q.best) atomicMin(&q.best, (int)ub);
 }
 
-// Cold path of a relaxation: candidate cost nc beats the target entry
-// (u, rank rS & 0xff, label td) read a moment ago; rS >> 8 is the subset.
-// Runs between relaxation batches, inline (a call's register convention
-// would cost the relaxation loop occupancy).  Returns 1 for an improvement
-// that survives the lower-bound test.
-__device__ __forceinline__ int grow_improve(Slot& q, long long V, uint32_t u, int rS, int nc, int td, int* dist) {
-  const int k = q.k, W = q.W, L = q.L, D = q.D, s = q.s, r = rS & 0xff;
+
+// Improvement path of a queued batch of candidates (nb <= GROW_QUEUE, at most
+// GROW_QUEUE / 32 per lane), each of which beat its target entry when the
+// relaxation loop read it.  It runs in phases, so that a lane's stores, mask
+// reads and mask atomics are in flight together instead of one candidate's
+// chain after another's: the atomicMin stores; for improvements, the touch of
+// a first finite entry, the lower bound and, at layer 1, the star upper bound;
+// then the dirty marks of the grow sources that survive the bound.  A
+// candidate that fails the bound is still stored (a real derivation cost:
+// later, costlier candidates for that state stop at the plain read), but
+// not marked.  The bound only decides whether a stored candidate is grown
+// from, so it is skipped for candidates that are not grow sources (cost
+// above best/2, or the last depth label).  Returns the improvements.
+__device__ __forceinline__ unsigned grow_cold(Slot& q, long long V, const int* qu, const int* qr, const int* qc,
+                                              int nb, int td, int* dist) {
+  constexpr int PER = GROW_QUEUE / 32;
+  const int lane = threadIdx.x & 31;
+  const int k = q.k, W = q.W, L = q.L, D = q.D, s = q.s;
   const bool hop = D >= 0;
-  const int best = *(volatile int*)&q.best;  // may be newer than the chunk's: only tighter
-  int32_t* trow = q.table + (long long)u * (W * L);
-  const long long tidx = (long long)(c_sub.loff[k][s] + r) * L;
-  // A candidate that fails the lower-bound test is still a real derivation
-  // cost: it is stored (unmarked, so never grown from) so that later,
-  // costlier candidates for this state stop at the plain read instead of
-  // re-running the bound.  The bound only decides whether a stored candidate
-  // is grown from, so it is skipped when the candidate is not a grow source
-  // anyway (cost above best/2, or the last depth label).
-  const bool source = 2LL * nc <= best && (!hop || td < D);
-  const bool pruned = s >= 2 && source && lb_prunes(q.sd + (long long)u * 8, k, W, rS >> 8, q.R1, q.lbtab, nc, best, dist);
-  const int old = atomicMin(&trow[tidx + td], nc);
-  if (old <= nc) return 0;
-  // a vertex with a finite entry is on the touched list already (whoever set
-  // the entry touched it), so only a first finite entry needs the flag read
-  if (old >= INF) touch(q, u);
-  if (pruned) return 1;
-  if (s == 1 && (!hop || td <= (D + 1) / 2)) star_bound(q, trow, k, L, hop ? D / 2 : 0, hop ? (D + 1) / 2 : 0);
-  if (source) {
-    if (!hop) mark_plain(q, V, u, r, nc);
-    else mark_dirty(q, V, u, r, td, td);
+  const int best = *(volatile int*)&q.best;
+  const int lo = c_sub.loff[k][s];
+  int old[PER];
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    const int x = lane + 32 * j;
+    old[j] = 0;
+    if (x < nb) {
+      int32_t* trow = q.table + (long long)(uint32_t)qu[x] * (W * L);
+      old[j] = atomicMin(&trow[(long long)(lo + (qr[x] & 0xff)) * L + td], qc[x]);
+    }
   }
-  return 1;
+  unsigned nimp = 0, mark = 0;
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    const int x = lane + 32 * j;
+    if (x < nb && old[j] > qc[x]) {
+      const uint32_t u = (uint32_t)qu[x];
+      const int rS = qr[x], nc = qc[x];
+      ++nimp;
+      if (old[j] >= INF) touch(q, u);
+      const bool source = 2LL * nc <= best && (!hop || td < D);
+      if (s >= 2 && source && lb_prunes(q.sd + (long long)u * 8, k, W, rS >> 8, q.R1, q.lbtab, nc, best, dist))
+        continue;
+      if (s == 1 && (!hop || td <= (D + 1) / 2))
+        star_bound(q, q.table + (long long)u * (W * L), k, L, hop ? D / 2 : 0, hop ? (D + 1) / 2 : 0);
+      if (source) mark |= 1u << j;
+    }
+  }
+  // dirty marks of the surviving sources: the mask words first (within a
+  // pass bits are only set, so a bit seen set needs no atomic), then the
+  // atomics, then the appends
+  unsigned long long om[PER];
+  int mi[PER];
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    const int x = lane + 32 * j;
+    om[j] = 1ull;
+    mi[j] = 0;
+    if ((mark >> j) & 1u) {
+      mi[j] = hop ? td : (qc[x] < q.T ? 0 : 1);
+      om[j] = *(volatile unsigned long long*)&q.mask[(long long)mi[j] * V + (uint32_t)qu[x]];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    const int x = lane + 32 * j;
+    if ((mark >> j) & 1u) {
+      const int r = qr[x] & 0xff;
+      if ((om[j] >> r) & 1ull) om[j] = 1ull;
+      else om[j] = atomicOr(&q.mask[(long long)mi[j] * V + (uint32_t)qu[x]], 1ull << r);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    if (!((mark >> j) & 1u)) continue;
+    const int x = lane + 32 * j;
+    const uint32_t u = (uint32_t)qu[x];
+    const int qi = hop ? td : (mi[j] == 0 ? (q.cur ^ 1) : q.fcur);
+    if (om[j] == 0ull) {
+      const int pos = atomicAdd(&q.qcount[qi], 1);
+      if (pos < V) q.queue[(long long)qi * V + pos] = u;
+      else q.err = ERR_QUEUE_CAP;
+    }
+    if (!hop && mi[j] == 1 && qc[x] < *(volatile int*)&q.next_min) atomicMin(&q.next_min, qc[x]);
+  }
+  return nimp;
 }
 
 template <int GROW_LANES>
@@ -1167,39 +1224,38 @@ k_grow_t(Slot* slots, const Plan* plan, Graph g) {
       int p0 = 0;
       while (true) {
         int nb = 0;  // queued candidates (warp-uniform)
-        for (; p0 < npmax && nb <= GROW_QUEUE - 32; p0 += GROW_LANES) {
-          int nc = INF, rS = 0;
-          int2 a = make_int2(0, 0);
-          if (p0 + sl < npairs) {
-            a = __ldg(&g.adj[e]);
-            rS = gr[bi];
-            nc = gsv[bi] + a.y;
-            ++nrel32;
-            if (use_dead && ((q.dead[(uint32_t)a.x >> 5] >> (a.x & 31)) & 1u)) nc = INF;
+        // two pairs per lane per step: their adjacency and target reads are
+        // independent, so each lane keeps two random reads in flight
+        for (; p0 < npmax && nb <= GROW_QUEUE - 64; p0 += 2 * GROW_LANES) {
+          int nc0 = INF, rS0 = 0, nc1 = INF, rS1 = 0;
+          int2 a0 = make_int2(0, 0), a1 = make_int2(0, 0);
+          if (p0 + sl < npairs) { a0 = __ldg(&g.adj[e]); rS0 = gr[bi]; nc0 = gsv[bi] + a0.y; ++nrel32; }
+          e += qG; bi += rG; if (bi >= na) { bi -= na; ++e; }
+          if (p0 + GROW_LANES + sl < npairs) { a1 = __ldg(&g.adj[e]); rS1 = gr[bi]; nc1 = gsv[bi] + a1.y; ++nrel32; }
+          e += qG; bi += rG; if (bi >= na) { bi -= na; ++e; }
+          if (use_dead) {
+            if (nc0 < INF && ((q.dead[(uint32_t)a0.x >> 5] >> (a0.x & 31)) & 1u)) nc0 = INF;
+            if (nc1 < INF && ((q.dead[(uint32_t)a1.x >> 5] >> (a1.x & 31)) & 1u)) nc1 = INF;
           }
-          e += qG;
-          bi += rG;
-          if (bi >= na) { bi -= na; ++e; }
-          bool imp = false;
-          if (nc < INF) {
-            const int32_t* trow = q.table + (long long)a.x * rowlen;
-            const long long tidx = (long long)(lo + (rS & 0xff)) * L;
-            int cv = trow[tidx + td];
-            for (int l = 0; l < td; ++l) cv = imin(cv, trow[tidx + l]);
-            imp = nc < cv;
+          int cv0 = INF, cv1 = INF;
+          if (nc0 < INF) {
+            const int32_t* trow = q.table + (long long)a0.x * rowlen + (long long)(lo + (rS0 & 0xff)) * L;
+            cv0 = trow[td]; for (int l = 0; l < td; ++l) cv0 = imin(cv0, trow[l]);
           }
-          const unsigned im = __ballot_sync(0xffffffffu, imp);
-          if (imp) {
-            const int x = nb + __popc(im & ((1u << lane) - 1));
-            s_qu[wib][x] = a.x;
-            s_qr[wib][x] = rS;
-            s_qc[wib][x] = nc;
+          if (nc1 < INF) {
+            const int32_t* trow = q.table + (long long)a1.x * rowlen + (long long)(lo + (rS1 & 0xff)) * L;
+            cv1 = trow[td]; for (int l = 0; l < td; ++l) cv1 = imin(cv1, trow[l]);
           }
-          nb += __popc(im);
+          const bool imp0 = nc0 < cv0, imp1 = nc1 < cv1;
+          const unsigned im0 = __ballot_sync(0xffffffffu, imp0);
+          if (imp0) { const int x = nb + __popc(im0 & ((1u << lane) - 1)); s_qu[wib][x] = a0.x; s_qr[wib][x] = rS0; s_qc[wib][x] = nc0; }
+          nb += __popc(im0);
+          const unsigned im1 = __ballot_sync(0xffffffffu, imp1);
+          if (imp1) { const int x = nb + __popc(im1 & ((1u << lane) - 1)); s_qu[wib][x] = a1.x; s_qr[wib][x] = rS1; s_qc[wib][x] = nc1; }
+          nb += __popc(im1);
         }
         __syncwarp();
-        for (int x = lane; x < nb; x += 32)
-          nimp += grow_improve(q, g.V, (uint32_t)s_qu[wib][x], s_qr[wib][x], s_qc[wib][x], td, dist);
+        nimp += grow_cold(q, g.V, s_qu[wib], s_qr[wib], s_qc[wib], nb, td, dist);
         __syncwarp();
         if (p0 >= npmax) break;
       }
