@@ -634,7 +634,7 @@ def main():
                    "per-query DP tables (GBs per step) exceed L2",
                    "tuning": {"file": os.path.relpath(tuning_file, ROOT) if tuning_file else None,
                               "params": {k: v for k, v in eng.get_tuning().items()
-                                         if k in ("grow_lanes", "rounds_per_poll", "max_slots")}}},
+                                         if k in ("grow_lanes", "rounds_per_poll", "max_slots", "overlap")}}},
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "gpu_launches": launches,

@@ -157,11 +157,15 @@ class Engine {
     tuning_.grow_lanes = GROW_LANES_DEFAULT;
     tuning_.rounds_per_poll = rounds_per_poll_;
     tuning_.max_slots = max_slots_;
+    tuning_.overlap = 1;
     for (int k = 0; k <= MAXK; ++k) {
       tuning_.chunk_pairs[k][0] = tuning_.chunk_pairs[k][1] = 1024;
       tuning_.bucket_mult[k] = 1;
     }
     GST_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    GST_CUDA(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking));  // the grow branch (overlap = 2)
+    GST_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+    GST_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
     SubsetTables st;
     fill_subset_tables(st);
     GST_CUDA(cudaMemcpyToSymbol(c_sub, &st, sizeof st));
@@ -200,6 +204,9 @@ class Engine {
     for (auto* p : {(void*)h_status_, (void*)h_list_, (void*)h_slot_, (void*)h_harv_, (void*)h_wedges_})
       if (p) cudaFreeHost(p);
     if (stream_) cudaStreamDestroy(stream_);
+    if (stream2_) cudaStreamDestroy(stream2_);
+    if (ev_fork_) cudaEventDestroy(ev_fork_);
+    if (ev_join_) cudaEventDestroy(ev_join_);
     d_slots_ = nullptr;
     arena_ = nullptr;
     device_ = -1;
@@ -367,6 +374,7 @@ class Engine {
     if (busy_) return fail(GST_E_STATE, "tuning: engine is serving");
     if (t.grow_lanes && t.grow_lanes != 8 && t.grow_lanes != 16 && t.grow_lanes != 32)
       return fail(GST_E_INVALID, "tuning: grow_lanes must be 8, 16 or 32");
+    if (t.overlap < 0 || t.overlap > 2) return fail(GST_E_INVALID, "tuning: overlap must be 1 or 2");
     if (t.rounds_per_poll < 0 || t.max_slots < 0 || t.max_slots > MAXSLOTS)
       return fail(GST_E_INVALID, "tuning: rounds_per_poll or max_slots out of range");
     for (int k = 0; k <= MAXK; ++k) {
@@ -375,6 +383,7 @@ class Engine {
         return fail(GST_E_INVALID, "tuning: chunk_pairs or bucket_mult out of range");
     }
     if (t.grow_lanes) tuning_.grow_lanes = t.grow_lanes;
+    if (t.overlap) tuning_.overlap = t.overlap;
     if (t.rounds_per_poll) tuning_.rounds_per_poll = rounds_per_poll_ = t.rounds_per_poll;
     if (t.max_slots) tuning_.max_slots = max_slots_ = t.max_slots;
     for (int k = 0; k <= MAXK; ++k) {
@@ -675,24 +684,38 @@ class Engine {
     return g;
   }
 
+  // One round.  The merge branch (lbprep, merge) and the grow branch (prep,
+  // ctl_b, grow) touch disjoint slots: with overlap = 2 they are forked onto
+  // two streams after ctl_a and joined before the next round.
   void enqueue_round(cudaStream_t st, int i) {
     Graph g = graph();
     const int grid = num_sms_ * 4;
+    const bool fork = tuning_.overlap == 2;
     k_ctl_a<<<1, MAXSLOTS, 0, st>>>(d_slots_, max_slots_, d_plan_, d_status_);
+    cudaStream_t sg = st;
+    if (fork) {
+      cudaEventRecord(ev_fork_, st);
+      cudaStreamWaitEvent(stream2_, ev_fork_, 0);
+      sg = stream2_;
+    }
     k_lbprep<<<std::min(max_slots_, 256), 256, 0, st>>>(d_slots_, d_plan_, g);
     if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 0], st, cudaEventRecordExternal);
     k_merge_t<false><<<grid, MERGE_THREADS, 0, st>>>(d_slots_, d_plan_, g);
     k_merge_t<true><<<grid, MERGE_THREADS, 0, st>>>(d_slots_, d_plan_, g);
     if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 1], st, cudaEventRecordExternal);
-    k_prep<<<grid, 256, 0, st>>>(d_slots_, d_plan_, g);
-    k_ctl_b<<<1, MAXSLOTS, 0, st>>>(d_slots_, d_plan_, 32 / tuning_.grow_lanes);
-    if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 2], st, cudaEventRecordExternal);
+    k_prep<<<grid, 256, 0, sg>>>(d_slots_, d_plan_, g);
+    k_ctl_b<<<1, MAXSLOTS, 0, sg>>>(d_slots_, d_plan_, 32 / tuning_.grow_lanes);
+    if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 2], sg, cudaEventRecordExternal);
     switch (tuning_.grow_lanes) {
-      case 8: k_grow_t<8><<<grow_grid_[0], GROW_WARPS * 32, 0, st>>>(d_slots_, d_plan_, g); break;
-      case 32: k_grow_t<32><<<grow_grid_[2], GROW_WARPS * 32, 0, st>>>(d_slots_, d_plan_, g); break;
-      default: k_grow_t<16><<<grow_grid_[1], GROW_WARPS * 32, 0, st>>>(d_slots_, d_plan_, g); break;
+      case 8: k_grow_t<8><<<grow_grid_[0], GROW_WARPS * 32, 0, sg>>>(d_slots_, d_plan_, g); break;
+      case 32: k_grow_t<32><<<grow_grid_[2], GROW_WARPS * 32, 0, sg>>>(d_slots_, d_plan_, g); break;
+      default: k_grow_t<16><<<grow_grid_[1], GROW_WARPS * 32, 0, sg>>>(d_slots_, d_plan_, g); break;
     }
-    if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 3], st, cudaEventRecordExternal);
+    if (profile_) cudaEventRecordWithFlags(ev_prof_[4 * i + 3], sg, cudaEventRecordExternal);
+    if (fork) {
+      cudaEventRecord(ev_join_, stream2_);
+      cudaStreamWaitEvent(st, ev_join_, 0);
+    }
   }
 
   gst_status launch_rounds() {
@@ -879,6 +902,8 @@ class Engine {
   int max_slots_ = 256;
   int rounds_per_poll_ = 8;
   cudaStream_t stream_ = nullptr;
+  cudaStream_t stream2_ = nullptr;
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   Slot* d_slots_ = nullptr;
   Plan* d_plan_ = nullptr;
   SlotStatus* d_status_ = nullptr;

@@ -76,7 +76,8 @@ class _Profile(ctypes.Structure):
 
 class _Tuning(ctypes.Structure):
     _fields_ = [("grow_lanes", ctypes.c_int), ("rounds_per_poll", ctypes.c_int), ("max_slots", ctypes.c_int),
-                ("chunk_pairs", (ctypes.c_int * 2) * (MAX_K + 1)), ("bucket_mult", ctypes.c_int * (MAX_K + 1))]
+                ("chunk_pairs", (ctypes.c_int * 2) * (MAX_K + 1)), ("bucket_mult", ctypes.c_int * (MAX_K + 1)),
+                ("overlap", ctypes.c_int)]
 
 
 class _Stats(ctypes.Structure):
@@ -318,12 +319,12 @@ class Engine:
     def get_tuning(self) -> dict:
         """Launch and scheduling parameters (gst_tuning) as a dict:
         grow_lanes, rounds_per_poll, max_slots, chunk_pairs[k] = [plain, D],
-        bucket_mult[k]."""
+        bucket_mult[k], overlap (1 serial, 2 merge and grow on two streams)."""
         t = _Tuning()
         _check(self._lib.gst_engine_get_tuning(self._h, ctypes.byref(t)), "get_tuning")
         return {"grow_lanes": t.grow_lanes, "rounds_per_poll": t.rounds_per_poll, "max_slots": t.max_slots,
                 "chunk_pairs": [[t.chunk_pairs[k][0], t.chunk_pairs[k][1]] for k in range(MAX_K + 1)],
-                "bucket_mult": [t.bucket_mult[k] for k in range(MAX_K + 1)]}
+                "bucket_mult": [t.bucket_mult[k] for k in range(MAX_K + 1)], "overlap": t.overlap}
 
     def set_tuning(self, tuning: dict) -> None:
         """Sets the parameters present in `tuning` (same keys as get_tuning;
@@ -332,6 +333,7 @@ class Engine:
         t.grow_lanes = int(tuning.get("grow_lanes", 0))
         t.rounds_per_poll = int(tuning.get("rounds_per_poll", 0))
         t.max_slots = int(tuning.get("max_slots", 0))
+        t.overlap = int(tuning.get("overlap", 0))
         for k, pair in enumerate(tuning.get("chunk_pairs", [])[: MAX_K + 1]):
             t.chunk_pairs[k][0], t.chunk_pairs[k][1] = int(pair[0]), int(pair[1])
         for k, m in enumerate(tuning.get("bucket_mult", [])[: MAX_K + 1]):

@@ -6,7 +6,8 @@ then writes them to a parameter file that gst_b200.Engine.load_tuning (and
 bench.py) apply:
 
 * engine-wide (timed on the whole batch): lanes per grow chunk {8, 16, 32},
-  device rounds between host polls {4, 8, 16, 32}, queries resident at once;
+  merge and grow of a round in sequence or on two streams, device rounds
+  between host polls {4, 8, 16, 32}, queries resident at once;
 * per query class (timed on that class's queries alone): (edge, set) pairs
   per grow chunk by (k, plain / D-bounded) {256 .. 4096}, and for plain
   queries the cost-bucket width as a multiple of the typical lightest edge
@@ -35,6 +36,7 @@ import time
 from .clocks import ClockSampler
 
 GROW_LANES = (8, 16, 32)
+OVERLAP = (1, 2)
 ROUNDS_PER_POLL = (4, 8, 16, 32)
 CHUNK_PAIRS = (256, 512, 1024, 2048, 4096)
 BUCKET_MULT = (1, 2, 4, 8)
@@ -107,6 +109,8 @@ class Tuner:
             self.log(f"pass {p + 1}: engine-wide parameters on {len(all_idx)} queries")
             tun["grow_lanes"], _ = self._descend(all_idx, "grow_lanes", GROW_LANES, tun["grow_lanes"],
                                                  lambda v: {**tun, "grow_lanes": v}, "all")
+            tun["overlap"], _ = self._descend(all_idx, "overlap", OVERLAP, tun["overlap"],
+                                              lambda v: {**tun, "overlap": v}, "all")
             tun["rounds_per_poll"], _ = self._descend(all_idx, "rounds_per_poll", ROUNDS_PER_POLL,
                                                       tun["rounds_per_poll"],
                                                       lambda v: {**tun, "rounds_per_poll": v}, "all")

@@ -145,6 +145,9 @@ typedef struct {
                                         [0] plain / [1] diameter-bounded (default 1024) */
   int bucket_mult[GST_MAX_K + 1];    /* plain grows: cost-bucket width = this many times
                                         the typical lightest edge, by k (default 1) */
+  int overlap;         /* 1: a round's merge and grow run one after the other (default);
+                          2: they run as two branches of the round graph, on two streams
+                          (they touch disjoint slots), so their kernels can share the GPU */
 } gst_tuning;
 
 gst_status gst_engine_set_tuning(gst_engine* e, const gst_tuning* t);
