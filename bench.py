@@ -463,7 +463,7 @@ def main():
     ap.add_argument("--workload", default="c4", choices=sorted(WORKLOADS) + ["c5"],
                     help="c5: the serving loop on the C4 graph")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--single-per-class", type=int, default=3,
+    ap.add_argument("--single-per-class", type=int, default=10,
                     help="queries of each (k, plain / D-bounded) class timed one per call")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=0, help="queries per step (0: the workload's count)")
