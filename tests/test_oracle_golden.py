@@ -79,3 +79,32 @@ def test_c2_fixture_regenerates_and_pins_the_restatement(golden):
     qs, want = fx["queries"]["5"], fx["reference"]["prunedpp"]["5"]
     for ids, w in zip(qs[:2], want[:2]):
         assert oracle.prunedpp(g, gr, ids)[0] == w
+
+
+@pytest.mark.parametrize("name", ["c3", "c4"])
+def test_benchmark_size_fixtures_reproduce(name):
+    """The C3 / C4 fixtures (made by tests/golden/make_golden_large.py from the
+    reference binaries) still describe what the generator builds, and their
+    queries are the workload's own queries at the recorded indices."""
+    import json
+    import os
+    import sys
+    from gst_b200 import datagen as dg
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, here)
+    import make_golden as mg
+    with open(os.path.join(here, f"{name}.json")) as f:
+        fx = json.load(f)
+    wl = dg.config_c4(1, n_queries=300) if name == "c4" else dg.config_c3(1, n_queries=300)
+    assert mg.checksum(wl.graph, wl.groups) == fx["checksum"]
+    pinned = 0
+    for c in fx["cells"]:
+        if not c.get("costs"):
+            assert c.get("not_pinned")
+            continue
+        for i, q, cost in zip(c["idx"], c["queries"], c["costs"]):
+            ids, D = wl.queries[i]
+            assert ids.tolist() == q and D == c["D"] and len(q) == c["k"]
+            assert cost == oracle.INF or 0 < cost < oracle.INF
+            pinned += 1
+    assert pinned >= (130 if name == "c4" else 18)
