@@ -238,11 +238,17 @@ gst_status gst_engine_profile(gst_engine* e, gst_profile* out);
  * All scratch lives in a file-scope static device array of
  * GST_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
  * exit; a query whose scratch would exceed it fails with GST_E_NOMEM.  Calls
- * share that array, so calls that overlap on the GPU race and must be
- * serialised by the caller.  The first call on a device performs a one-time
- * set-up on it and should come before any stream capture.  `stream` is a
- * cudaStream_t (NULL: the legacy default stream); the call returns after the
- * stream has finished the query. */
+ * share that array and it keeps the last call's contents: each call clears
+ * what must start cleared, and the library serialises the calls of one
+ * process (a call holds a lock until its work has finished), since calls that
+ * overlapped on the GPU would race on the array.  The first call on a device
+ * performs a one-time set-up on it (the array's device address, the subset
+ * tables) and should come before any stream capture; a context that was reset
+ * and re-created since is detected and set up again.  Device waits are
+ * bounded by GST_WATCHDOG_S seconds (environment, default 120): a wait that
+ * runs out fails the call with GST_E_CUDA and later calls on that device are
+ * refused.  `stream` is a cudaStream_t (NULL: the legacy default stream); the
+ * call returns after the stream has finished the query. */
 gst_status gst_solve_noalloc(int64_t V, int64_t E, const int64_t* d_rowptr, const int32_t* d_adj,
                              int64_t n_groups, const int64_t* d_group_ptr,
                              const int32_t* d_group_members, const int32_t* group_ids, int k,
