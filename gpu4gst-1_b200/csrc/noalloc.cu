@@ -14,9 +14,10 @@
 // The array is part of this library's device image: every GPU that loads the
 // library holds it until the process exits.  All calls share it and it keeps
 // the previous call's contents, so each call re-initialises what must start
-// cleared; calls that overlap on the GPU (different host threads, or
-// different streams of one device) race on it and must be serialised by the
-// caller.  The first call on a device does a one-time set-up on that device
+// cleared.  Calls that overlapped on the GPU would race on it, so a call holds
+// a process-wide lock from its first device operation until its work has
+// finished (calls from several host threads, or for several streams, run one
+// after another).  The first call on a device does a one-time set-up on that device
 // (symbol address lookup, subset tables); make that first
 // call before any stream capture.  Every call checks a token that the set-up
 // wrote into this library's device memory: a context that was reset and
