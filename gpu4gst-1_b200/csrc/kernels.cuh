@@ -28,8 +28,10 @@
 //   * after an untruncated layer 1, a missing singleton entry means the group
 //     is out of reach, so every (v, S) containing it is skipped.
 // All kernels run on a fixed grid and read their work sizes from device
-// memory, so a round (ctl_a, lbprep, merge, prep, ctl_b, grow) can be captured
-// once in a CUDA graph and replayed.
+// memory, so a round (ctl_a, then the merge branch lbprep, merge, merge_wide
+// and the grow branch prep, ctl_b, grow, which touch disjoint slots) can be
+// captured once in a CUDA graph and replayed.  Finished slots get k_witness
+// (tree rebuild) and k_validate (tree check).
 #pragma once
 #include <cuda_runtime.h>
 
