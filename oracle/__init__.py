@@ -38,9 +38,11 @@ def _load():
         lib.oracle_prunedpp.argtypes = common + [P, ctypes.c_int, ctypes.POINTER(Result)]
         lib.oracle_dpbf.argtypes = common + [P, ctypes.c_int, ctypes.POINTER(Result)]
         lib.oracle_hop.argtypes = common + [ctypes.c_int, P, ctypes.c_int, ctypes.POINTER(Result)]
+        lib.oracle_hop_lean.argtypes = common + [ctypes.c_int, P, ctypes.c_int, ctypes.POINTER(Result)]
         lib.oracle_validate.argtypes = common + [P, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
                                                  ctypes.c_int]
-        for f in (lib.oracle_prunedpp, lib.oracle_dpbf, lib.oracle_hop, lib.oracle_validate):
+        for f in (lib.oracle_prunedpp, lib.oracle_dpbf, lib.oracle_hop, lib.oracle_hop_lean,
+                  lib.oracle_validate):
             f.restype = ctypes.c_int
         _lib = lib
     return _lib
@@ -79,6 +81,13 @@ def dpbf(graph, groups, query):
 def hop(graph, groups, query, D):
     """HOP_cpu restatement (diameter bound D); returns (cost, edges, root, pops)."""
     return _solve(_load().oracle_hop, graph, groups, query, extra=(int(D),))
+
+
+def hop_lean(graph, groups, query, D):
+    """HOP_cpu restatement holding 4 bytes per (vertex, set, hop) state and
+    rebuilding the tree from the costs; same answers as hop(), for graphs
+    where hop()'s node table does not fit.  Returns (cost, edges, root, pops)."""
+    return _solve(_load().oracle_hop_lean, graph, groups, query, extra=(int(D),))
 
 
 def validate(graph, groups, query, edges, root, cost, D=-1) -> int:

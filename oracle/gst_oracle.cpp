@@ -714,6 +714,132 @@ int oracle_hop(int64_t V, const int64_t* rowptr, const int32_t* col, const int32
   return 0;
 }
 
+// HOP_cpu (code/D-PrunedDP++/include/CPUHOP.h:107-288) with 4 bytes per
+// (v, p, d) state instead of a 44-byte node: the same Dijkstra with lazy
+// deletion, the same grow and merge rules and the same stop at the first
+// settled full set, but no back-pointers.  The tree is rebuilt from the cost
+// table by exact equalities (a base state, a grow edge u with
+// cost(u, p, d-1) + w = cost, or a merge (p1, d1) + (p2, d2) = cost); every
+// finite entry was set from a settled state by one of those rules, so a
+// witness always exists.  Reported cost: the weight of the de-duplicated edge
+// set, as the reference reports it (exp_CPU_Hop.h:146); 100000 when
+// infeasible.  Exists for sizes where the reference's table does not fit in
+// memory (4M vertices, k = 7: 88 to 155 GB); pinned against the reference
+// wherever that one runs.
+int oracle_hop_lean(int64_t V, const int64_t* rowptr, const int32_t* col, const int32_t* w,
+                    const int64_t* gptr, const int32_t* gmem, int64_t ngroups, const int32_t* query,
+                    int k_in, int D, int32_t* edges, int edge_cap, oracle_result* out) {
+  if (!out || V <= 0 || k_in <= 0 || D < 0) return -1;
+  Csr g{V, rowptr, col, w};
+  Groups gr{gptr, gmem, ngroups};
+  std::vector<int> qg = distinct_groups(query, k_in);
+  const int k = (int)qg.size();
+  if (k > 16) return -1;
+  const int full = (1 << k) - 1, W = 1 << k, DD = D + 1;
+  const size_t NS = (size_t)V * W * DD;
+  std::vector<int> cost(NS, kInf);
+  auto id = [&](size_t v, int p, int d) { return ((size_t)v * W + p) * DD + d; };
+  std::vector<int> gs = vertex_groupsets(g, gr, qg);
+  struct QE {
+    int cost;
+    uint32_t v;
+    uint16_t p;
+    uint8_t d;
+    bool operator>(const QE& o) const { return cost > o.cost; }
+  };
+  std::priority_queue<QE, std::vector<QE>, std::greater<QE>> q;
+  for (int64_t v = 0; v < V; ++v)
+    for (int i = 0; i < k; ++i)
+      if (gs[v] >> i & 1) {
+        cost[id(v, 1 << i, 0)] = 0;
+        q.push({0, (uint32_t)v, (uint16_t)(1 << i), 0});
+      }
+  out->pops = 0;
+  out->feasible = 0;
+  out->root = -1;
+  int64_t rv = -1;
+  int rd = -1;
+  while (!q.empty()) {
+    const QE e = q.top();
+    q.pop();
+    out->pops++;
+    if (e.cost != cost[id(e.v, e.p, e.d)]) continue;
+    if (e.p == full) {
+      rv = e.v;
+      rd = e.d;
+      break;
+    }
+    if (e.d < D)
+      for (int64_t j = rowptr[e.v]; j < rowptr[e.v + 1]; ++j) {
+        const size_t t = id(col[j], e.p, e.d + 1);
+        if (cost[t] > e.cost + w[j]) {
+          cost[t] = e.cost + w[j];
+          q.push({cost[t], (uint32_t)col[j], e.p, (uint8_t)(e.d + 1)});
+        }
+      }
+    for (int p2 = 1; p2 <= full; ++p2) {
+      if (p2 & e.p) continue;
+      for (int d2 = 0; d2 <= D - e.d; ++d2) {
+        const int c2 = cost[id(e.v, p2, d2)];
+        if (c2 >= kInf) continue;
+        const int pu = e.p | p2, nd = std::max<int>(e.d, d2);
+        const size_t t = id(e.v, pu, nd);
+        if (cost[t] > e.cost + c2) {
+          cost[t] = e.cost + c2;
+          q.push({cost[t], e.v, (uint16_t)pu, (uint8_t)nd});
+        }
+      }
+    }
+  }
+  if (rv < 0) {
+    out->cost = kInf;
+    out->n_edges = 0;
+    return 0;
+  }
+  EdgeSet sol;
+  struct Item {
+    int64_t v;
+    int p, d;
+  };
+  std::vector<Item> st{{rv, full, rd}};
+  while (!st.empty()) {
+    const Item it = st.back();
+    st.pop_back();
+    sol.add_vertex((int)it.v);
+    const int c = cost[id(it.v, it.p, it.d)];
+    if (c == 0 && it.d == 0 && (it.p & gs[it.v]) == it.p && __builtin_popcount(it.p) == 1) continue;
+    bool found = false;
+    if (it.d > 0)
+      for (int64_t j = rowptr[it.v]; j < rowptr[it.v + 1] && !found; ++j) {
+        const int cu = cost[id(col[j], it.p, it.d - 1)];
+        if (cu < kInf && cu + w[j] == c) {
+          sol.add_edge(col[j], (int)it.v);
+          st.push_back({col[j], it.p, it.d - 1});
+          found = true;
+        }
+      }
+    for (int p1 = (it.p - 1) & it.p; p1 > 0 && !found; p1 = (p1 - 1) & it.p) {
+      const int p2 = it.p ^ p1;
+      for (int d1 = 0; d1 <= it.d && !found; ++d1)
+        for (int d2 = 0; d2 <= D - d1 && !found; ++d2) {
+          if (std::max(d1, d2) != it.d) continue;
+          const int a = cost[id(it.v, p1, d1)], b = cost[id(it.v, p2, d2)];
+          if (a < kInf && b < kInf && a + b == c) {
+            st.push_back({it.v, p1, d1});
+            st.push_back({it.v, p2, d2});
+            found = true;
+          }
+        }
+    }
+    if (!found) return -2;  // an entry without a witness: the table is inconsistent
+  }
+  out->feasible = 1;
+  out->root = (int)rv;
+  out->cost = sol.weight(g);
+  write_edges(sol, g, edges, edge_cap, &out->n_edges);
+  return 0;
+}
+
 // Checks a solution.  Returns 0 if valid, else a positive code:
 //   1 an edge is not in the graph or has a different weight
 //   2 the edge set is not a tree (cycle or disconnected)

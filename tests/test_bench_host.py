@@ -29,6 +29,7 @@ def test_fixture_parity_accepts_the_reference_costs_and_rejects_one_change(c4):
             costs[i] = want
     got = bench.fixture_parity("c4", c4, costs)
     assert got["equal"] and got["queries_checked"] == sum(x is not None for x in costs)
+    assert sum(got["by_program"].values()) == got["queries_checked"]
     i = next(i for i, x in enumerate(costs) if x is not None and x < 100000)
     costs[i] += 1  # a mistake planted in the checked values, on the CPU
     with pytest.raises(AssertionError):

@@ -134,8 +134,10 @@ def _large_fixture(name):
 def test_benchmark_size_costs_equal_the_reference_binaries(name):
     """C4 (4M vertices, the headline workload) and C3 (1M vertices, k=7 with
     D in {2..5}): every pinned query of every (k, D) cell equals the cost the
-    reference PrunedDP++ / D-PrunedDP++ printed, solved as one batch; the first
-    query of each cell also one per call; every tree passes the checker."""
+    reference PrunedDP++ / D-PrunedDP++ printed (for C4's k=7 D-bounded cells,
+    whose reference table does not fit in memory, the cost of the HOP_cpu
+    restatement oracle.hop_lean), solved as one batch; the first query of each
+    cell also one per call; every tree passes the checker."""
     fx, wl, cells = _large_fixture(name)
     e = gst_b200.Engine(device=0, max_rounds=2000000)
     e.load_graph(wl.graph.rowptr, wl.graph.col, wl.graph.w)

@@ -44,6 +44,21 @@ def test_hop_restatement_matches_reference(golden, name):
             assert cost == w, (name, ids, h["D"], cost, w)
 
 
+@pytest.mark.parametrize("name", ["toy60", "s3000", "c1", "edge"])
+def test_lean_hop_restatement_matches_reference(golden, name):
+    """The 4-bytes-per-state HOP restatement (which pins the C4 cells whose
+    reference table does not fit) gives the reference's cost on every cell,
+    and its rebuilt tree keeps the hop bound."""
+    fx, g, gr = golden(name)
+    for h in fx["reference"]["hop"]:
+        qs = fx["queries"][str(h["k"])][: h["n"]]
+        for ids, w in zip(qs, h["costs"]):
+            cost, edges, root, _ = oracle.hop_lean(g, gr, ids, h["D"])
+            assert cost == w, (name, ids, h["D"], cost, w)
+            if cost < oracle.INF:
+                assert oracle.validate(g, gr, ids, edges, root, cost, h["D"]) == 0
+
+
 def test_hop_properties_on_oracle(golden):
     """Cost is non-increasing in D and reaches the plain optimum for large D."""
     fx, g, gr = golden("toy60")
@@ -102,6 +117,11 @@ def test_benchmark_size_fixtures_reproduce(name):
         if not c.get("costs"):
             assert c.get("not_pinned")
             continue
+        # who printed the costs: a reference binary, or (only for a cell the
+        # reference cannot run, with the reason recorded) the restatement
+        assert c["program"] in ("PrunedDP++", "D-PrunedDP++", "oracle.hop_lean")
+        if c["program"] == "oracle.hop_lean":
+            assert c["D"] >= 0 and c.get("reference_not_run")
         for i, q, cost in zip(c["idx"], c["queries"], c["costs"]):
             ids, D = wl.queries[i]
             assert ids.tolist() == q and D == c["D"] and len(q) == c["k"]
