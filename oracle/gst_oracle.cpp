@@ -14,6 +14,10 @@
 //                        pruning rules (code/PrunedDP++/include/CPUNONHOP.h:499-967)
 //   oracle_hop        -- diameter-bounded Dijkstra over (v, S, d)
 //                        (code/D-PrunedDP++/include/CPUHOP.h:107-288)
+//   oracle_hop_lean   -- the same search with 4 bytes per (v, S, d) state and
+//                        the tree rebuilt from the costs, for graphs where the
+//                        node table does not fit (4M vertices, k = 7); pinned
+//                        against the reference wherever that one runs
 //   oracle_dpbf       -- unpruned exact DPBF (Dijkstra over (v, S)); ground
 //                        truth used to check that the pruned solvers are exact
 //   oracle_validate   -- solution check: edges exist with their weights, the

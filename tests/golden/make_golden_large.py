@@ -55,13 +55,13 @@ import oracle  # noqa: E402
 SUBSETS = {
     "c4": {(3, -1): 52, (5, -1): 24, (7, -1): 24,
            (3, 2): 10, (3, 3): 10, (3, 4): 10, (3, 5): 10,
-           (5, 2): 2, (5, 3): 2, (5, 4): 2, (5, 5): 2,
+           (5, 2): 6, (5, 3): 6, (5, 4): 6, (5, 5): 6,
            (7, 2): 0, (7, 3): 0, (7, 4): 0, (7, 5): 0},
     "c3": {(7, 2): 6, (7, 3): 6, (7, 4): 3, (7, 5): 3},
 }
 # Cells pinned by the restatement (--restatement): the first n queries of
 # each cell the reference cannot run.
-LEAN_SUBSETS = {"c4": {(7, 2): 6, (7, 3): 6, (7, 4): 4, (7, 5): 4}}
+LEAN_SUBSETS = {"c4": {(7, 2): 6, (7, 3): 6, (7, 4): 6, (7, 5): 6}}
 LEAN_PROGRAM = "oracle.hop_lean"
 PLAIN_PER_JOB = 4  # plain queries per process (amortises the graph load)
 
@@ -87,8 +87,9 @@ def mem_bytes(wl, k, D):
 
 def lean_mem_bytes(wl, k, D):
     """Resident memory of one restatement process: the graph arrays (mapped),
-    the int32 cost table and its heap, taken as half the table again."""
-    return 1.5 * wl.graph.V * (1 << k) * (D + 1) * 4 + 2e9
+    the int32 cost table and its heap (measured under a fifth of the table
+    for C4 k=7 D=5; budgeted at a quarter)."""
+    return 1.25 * wl.graph.V * (1 << k) * (D + 1) * 4 + 1e9
 
 
 def save_arrays(d, wl):
@@ -166,18 +167,26 @@ def run_jobs(jobs, procs, mem_budget, log):
 
 def lean_jobs(name, wl, d, k, D, n, fx, save, wlock, log):
     """Jobs that pin the first n queries of cell (k, D) with the restatement,
-    one process per query."""
+    one process per query; queries an earlier restatement cell of the same
+    inputs already pinned are kept, not rerun."""
     save_arrays(d, wl)
     queries = wl.queries
     idx = [i for i, (q, qd) in enumerate(queries) if len(q) == k and qd == D][:n]
+    old = next((c for c in fx["cells"] if (c["k"], c["D"]) == (k, D) and c.get("program") == LEAN_PROGRAM), None)
+    kept = {i: (c, t) for i, c, t in zip(old["idx"], old["costs"], old["oracle_time_s"])} if old else {}
     need = mem_bytes(wl, k, D) / 1e9
     cell = dict(k=k, D=D, idx=idx, queries=[queries[i][0].tolist() for i in idx],
                 costs=[None] * len(idx), oracle_time_s=[None] * len(idx), program=LEAN_PROGRAM,
                 reference_not_run=f"D-PrunedDP++ allocates its whole table up front: {need:.0f} GB "
                                   f"for k={k}, D={D} on {wl.graph.V:,} vertices")
-    pending = {"n": len(idx)}
+    for j, i in enumerate(idx):
+        if i in kept:
+            cell["costs"][j], cell["oracle_time_s"][j] = kept[i]
+    pending = {"n": sum(i not in kept for i in idx)}
     jobs = []
     for j, i in enumerate(idx):
+        if i in kept:
+            continue
         out = os.path.join(d, f"lean_{name}_k{k}_D{D}_{i}.json")
         argv = [sys.executable, os.path.abspath(__file__), "--lean-job", d, str(D),
                 ",".join(str(int(x)) for x in queries[i][0]), out]
@@ -229,17 +238,20 @@ def main():
             old = json.load(f)
         if old.get("checksum") == fx["checksum"]:
             fx["cells"] = [c for c in old.get("cells", []) if c.get("costs") or c.get("not_pinned")]
-    # with --restatement the not-pinned cells are the ones to redo; each keeps
-    # its record until its replacement is finished (a restatement cell smaller
-    # than its subset is redone)
+    # A cell smaller than its subset is extended: its pinned queries are kept
+    # and only the missing ones run.  With --restatement the not-pinned cells
+    # are the ones to redo; each keeps its record until its replacement is
+    # finished.
     lean = LEAN_SUBSETS.get(name, {})
 
     def finished(c):
-        if not args.restatement:
-            return True
+        key = (c["k"], c["D"])
         if c.get("program") == LEAN_PROGRAM:
-            return len(c["idx"]) >= lean.get((c["k"], c["D"]), 0)
-        return bool(c.get("costs"))
+            return not args.restatement or len(c["idx"]) >= lean.get(key, 0)
+        if c.get("costs"):
+            avail = sum(len(q) == c["k"] and qd == c["D"] for q, qd in queries)
+            return len(c["idx"]) >= min(SUBSETS[name].get(key, 0), avail)
+        return not args.restatement
     done_cells = {(c["k"], c["D"]) for c in fx["cells"] if finished(c)}
     wlock = threading.Lock()
 
@@ -280,45 +292,53 @@ def main():
             continue
         if not idx:
             continue
+        prog = "PrunedDP++" if D < 0 else "D-PrunedDP++"
+        old = next((c for c in fx["cells"] if (c["k"], c["D"]) == (k, D) and c.get("program") == prog
+                    and c.get("costs")), None)
+        kept = {i: (c, t) for i, c, t in zip(old["idx"], old["costs"], old["ref_time_s"])} if old else {}
+        cell.update(costs=[kept[i][0] if i in kept else None for i in idx],
+                    ref_time_s=[kept[i][1] if i in kept else None for i in idx], program=prog)
+        todo = [i for i in idx if i not in kept]  # the queries this run solves, in cell order
+        pos = {i: j for j, i in enumerate(idx)}
+        if not todo:
+            continue
         ensure_dataset()
-        # a data name per cell: symlinks to the shared graph and groups, the
-        # cell's queries as <data><k>.csv
-        data = f"{name}_k{k}_" + ("plain" if D < 0 else f"D{D}")
+        # a data name per cell (and per extension): symlinks to the shared
+        # graph and groups, the queries to solve as <data><k>.csv
+        data = f"{name}_k{k}_" + ("plain" if D < 0 else f"D{D}") + (f"_from{len(kept)}" if kept else "")
         for ext in (".in", ".g"):
             dst = os.path.join(d, data + ext)
             if not os.path.exists(dst):
                 os.symlink(os.path.join(d, name + ext), dst)
-        dg.write_queries(os.path.join(d, f"{data}{k}.csv"), [queries[i] for i in idx])
-        prog = "PrunedDP++" if D < 0 else "D-PrunedDP++"
+        dg.write_queries(os.path.join(d, f"{data}{k}.csv"), [queries[i] for i in todo])
         per = PLAIN_PER_JOB if D < 0 else 1
-        cell.update(costs=[None] * len(idx), ref_time_s=[None] * len(idx), program=prog)
         pending = {"n": 0}
-        for a in range(0, len(idx), per):
-            b = min(a + per, len(idx)) - 1
+        for a in range(0, len(todo), per):
+            b = min(a + per, len(todo)) - 1
             argv = [oracle.ref_binary(prog), "1" if D < 0 else "2", d + "/", data, str(k)]
             argv += ([str(D)] if D >= 0 else []) + [str(a), str(b)]
             tag = "CPU_nonHop" if D < 0 else "CPU_Hop"
             csv = os.path.join(d, "result", f"exp_{tag}_{data}_T{k}_" + (f"D{D}_" if D >= 0 else "") + f"{a}-{b}.csv")
             pending["n"] += 1
 
-            def done(job, cell=cell, a=a, csv=csv, pending=pending):
+            def done(job, cell=cell, a=a, csv=csv, pending=pending, todo=todo, pos=pos, k=k, D=D):
                 with open(csv) as f:
                     next(f)
                     rows = [ln.strip().split(",") for ln in f if ln.strip()]
                 with wlock:
                     for j, r in enumerate(rows):
-                        cell["costs"][a + j] = int(r[3])
-                        cell["ref_time_s"][a + j] = float(r[2])
+                        cell["costs"][pos[todo[a + j]]] = int(r[3])
+                        cell["ref_time_s"][pos[todo[a + j]]] = float(r[2])
                     pending["n"] -= 1
                     last = pending["n"] == 0
                     if last:
-                        fx["cells"].append(cell)
+                        fx["cells"] = [c for c in fx["cells"] if (c["k"], c["D"]) != (k, D)] + [cell]
                 log(f"{job['label']}: {[r[3] for r in rows]} in {job['wall']:.0f} s")
                 if last:
                     save()
 
             jobs.append(dict(argv=argv, cwd=d, mem=mem_bytes(wl, k, D), done=done,
-                             label=f"{name} k={k} D={D} queries {a}-{b}"))
+                             label=f"{name} k={k} D={D} queries {[todo[x] for x in range(a, b + 1)]}"))
     save()
     log(f"{len(jobs)} jobs, {args.procs} processes, {args.mem_gb} GB")
     run_jobs(jobs, args.procs, args.mem_gb * 1e9, log)
