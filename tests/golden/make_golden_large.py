@@ -57,7 +57,7 @@ SUBSETS = {
            (3, 2): 10, (3, 3): 10, (3, 4): 10, (3, 5): 10,
            (5, 2): 6, (5, 3): 6, (5, 4): 6, (5, 5): 6,
            (7, 2): 0, (7, 3): 0, (7, 4): 0, (7, 5): 0},
-    "c3": {(7, 2): 6, (7, 3): 6, (7, 4): 3, (7, 5): 3},
+    "c3": {(7, 2): 10, (7, 3): 10, (7, 4): 6, (7, 5): 6},
 }
 # Cells pinned by the restatement (--restatement): the first n queries of
 # each cell the reference cannot run.
