@@ -254,12 +254,20 @@ def run_ref_timed(exe: str, d: str, name: str, k: int, a: int, b: int, budget_s:
     return times, cut
 
 
+def sample_positions(n: int, per_k: int) -> list:
+    """per_k positions spread evenly over a class of n queries (0, n/per_k,
+    2n/per_k, ...): query times within a class spread over two orders of
+    magnitude, so the first queries alone are no fair sample."""
+    m = min(per_k, n)
+    return [j * n // m for j in range(m)]
+
+
 def cpu_reference_sample(name: str, per_k: int, budget_s: float = 300):
-    """The reference PrunedDP++ (oracle/_ref) on the first per_k plain
-    queries of each k of the workload, one single-threaded process per query,
-    all at once, each stopped budget_s seconds after its query started.
-    Returns per-class mean seconds per query (a stopped query counts with the
-    time it had run: a lower bound) and what ran."""
+    """The reference PrunedDP++ (oracle/_ref) on per_k plain queries of each
+    k of the workload, spread evenly over the class, one single-threaded
+    process per query, all at once, each stopped budget_s seconds after its
+    query started.  Returns per-class mean seconds per query (a stopped query
+    counts with the time it had run: a lower bound) and what ran."""
     import oracle
     exe = oracle.ref_binary("PrunedDP++")
     if not os.path.exists(exe):
@@ -267,7 +275,7 @@ def cpu_reference_sample(name: str, per_k: int, budget_s: float = 300):
     d = os.path.join(tempfile.gettempdir(), f"gstbench_{name}")
     os.makedirs(os.path.join(d, "result"), exist_ok=True)
     byk = write_dataset_files(name, d)
-    jobs = [(k, i) for k in sorted(byk) for i in range(min(per_k, len(byk[k])))]
+    jobs = [(k, i) for k in sorted(byk) for i in sample_positions(len(byk[k]), per_k)]
     out = [None] * len(jobs)
 
     def one(j):
@@ -287,7 +295,8 @@ def cpu_reference_sample(name: str, per_k: int, budget_s: float = 300):
             per.setdefault(k, []).append(cut)
             stopped += 1
     return {"per_k_s": {k: statistics.mean(v) for k, v in per.items()}, "queries": len(jobs),
-            "per_k": per_k, "stopped": stopped, "budget_s": budget_s}
+            "per_k": per_k, "stopped": stopped, "budget_s": budget_s,
+            "positions": {k: sample_positions(len(byk[k]), per_k) for k in sorted(byk)}}
 
 
 def cpu_mix_qps(per_k_s: dict, queries, cores: int):
@@ -485,7 +494,8 @@ def main():
     ap.add_argument("--serve-queries", type=int, default=10000, help="c5: queries per rate")
     ap.add_argument("--ref-budget", type=float, default=360.0,
                     help="reference arm: seconds each reference process runs after its first query")
-    ap.add_argument("--cpu-per-k", type=int, default=1, help="cpu_baseline: plain queries per k")
+    ap.add_argument("--cpu-per-k", type=int, default=3,
+                    help="cpu_baseline: plain queries per k, spread evenly over the class")
     ap.add_argument("--cpu-budget", type=float, default=300.0,
                     help="cpu_baseline: seconds a reference process may run its query")
     ap.add_argument("--tuning", default="auto",
@@ -676,7 +686,8 @@ def main():
             qps = cpu_mix_qps(smp["per_k_s"], wl.queries, cores)
             out["cpu_baseline"] = {
                 "value": qps, "unit": "queries/s", "cores": cores, "kind": "reference",
-                "sample": f"the first {smp['per_k']} plain queries of each k of this workload, one "
+                "sample": f"{smp['per_k']} plain queries of each k of this workload (spread evenly over "
+                          f"the class: positions {smp['positions']}), one "
                           f"single-threaded PrunedDP++ process each ({smp['queries']} at once, on host cores "
                           f"while the GPU steps ran); per-query time from the reference's progress lines "
                           f"(graph load excluded); {smp['stopped']} queries still running after "

@@ -59,3 +59,10 @@ def test_tuning_file_round_trip(tmp_path):
         committed = autotune.load(os.path.join(ROOT, "gpu4gst-1_b200", "tuning", f"{w}.json"))
         assert committed["grow_lanes"] in (8, 16, 32) and committed.get("overlap", 1) in (1, 2)
         assert len(committed["chunk_pairs"]) == 8 and len(committed["bucket_mult"]) == 8
+
+
+def test_cpu_sample_positions_spread_over_the_class():
+    assert bench.sample_positions(52, 3) == [0, 17, 34]
+    assert bench.sample_positions(60, 3) == [0, 20, 40]
+    assert bench.sample_positions(2, 3) == [0, 1]  # a class smaller than the sample
+    assert bench.sample_positions(60, 1) == [0]
