@@ -101,14 +101,19 @@ def arrays_checksum(g, gr) -> str:
 
 def fixture_parity(name: str, wl, costs) -> dict | None:
     """Compares the batch's costs with the reference costs committed in
-    tests/golden/<name>.json (the queries there are this workload's own, by
-    index).  Raises if one differs."""
-    path = os.path.join(ROOT, "tests", "golden", f"{name}.json")
-    if not os.path.exists(path):
-        return None
-    with open(path) as f:
-        fx = json.load(f)
-    if "cells" not in fx or fx.get("checksum") != arrays_checksum(wl.graph, wl.groups):
+    tests/golden/<name>.json, or <name>_batch.json (the queries there are this
+    workload's own, by index).  Raises if one differs."""
+    fx = None
+    for fn in (f"{name}.json", f"{name}_batch.json"):
+        path = os.path.join(ROOT, "tests", "golden", fn)
+        if not os.path.exists(path):
+            continue
+        with open(path) as f:
+            cand = json.load(f)
+        if "cells" in cand and cand.get("checksum") == arrays_checksum(wl.graph, wl.groups):
+            fx = cand
+            break
+    if fx is None:
         return None
     n = 0
     by_program = {}
@@ -122,7 +127,7 @@ def fixture_parity(name: str, wl, costs) -> dict | None:
             assert costs[i] == want, f"query {i} (k={c['k']}, D={c['D']}): {costs[i]} != {prog} {want}"
             n += 1
             by_program[prog] = by_program.get(prog, 0) + 1
-    return {"fixture": f"tests/golden/{name}.json", "queries_checked": n, "equal": True,
+    return {"fixture": f"tests/golden/{fn}", "queries_checked": n, "equal": True,
             "by_program": by_program,
             "against": "reference PrunedDP++ / D-PrunedDP++ costs; oracle.hop_lean (the HOP_cpu "
                        "restatement) only on cells whose reference table does not fit in memory"}

@@ -1,5 +1,9 @@
-"""Generates tests/golden/c3.json and c4.json: reference costs at the
-benchmark sizes, from the reference programs themselves.
+"""Generates tests/golden/c3.json, c4.json and c2_batch.json: reference
+costs at the benchmark sizes, from the reference programs themselves.
+
+C2_batch is the 170k-vertex k=5 workload's whole 300-query batch (BA m=20 +
+spanning path, w U[1,100], 3,000 groups Geom(8) in [2,200]), every query
+pinned by PrunedDP++.
 
 C3 is the 1M-vertex diameter-bounded k=7 workload (BA m=10, w U[1,1000],
 10,000 groups Geom(10) in [2,500], 300 queries with D in {2..5}); C4 is the
@@ -26,7 +30,7 @@ equals D-PrunedDP++ on every C3 cell and on the small fixtures.  Such cells
 name that program in "program", so a reader (and the benchmark's parity
 line) can tell them from cells the reference binaries printed.
 
-    python tests/golden/make_golden_large.py c4|c3 [--procs N] [--mem-gb G] [--restatement]
+    python tests/golden/make_golden_large.py c4|c3|c2 [--procs N] [--mem-gb G] [--restatement]
 """
 from __future__ import annotations
 
@@ -58,7 +62,11 @@ SUBSETS = {
            (5, 2): 6, (5, 3): 6, (5, 4): 6, (5, 5): 6,
            (7, 2): 0, (7, 3): 0, (7, 4): 0, (7, 5): 0},
     "c3": {(7, 2): 10, (7, 3): 10, (7, 4): 6, (7, 5): 6},
+    "c2": {(5, -1): 300},
 }
+# The C2 batch fixture is written beside the older tests/golden/c2.json (its
+# first 12 queries, in make_golden.py's format), not over it.
+FIXTURE_FILE = {"c2": "c2_batch"}
 # Cells pinned by the restatement (--restatement): the first n queries of
 # each cell the reference cannot run.
 LEAN_SUBSETS = {"c4": {(7, 2): 6, (7, 3): 6, (7, 4): 6, (7, 5): 6}}
@@ -69,6 +77,8 @@ PLAIN_PER_JOB = 4  # plain queries per process (amortises the graph load)
 def workload(name):
     if name == "c4":
         return dg.config_c4(1, n_queries=300), dict(config="c4", seed=1, n_queries=300)
+    if name == "c2":
+        return dg.config_c2(1, n_queries=300), dict(config="c2", seed=1, n_queries=300)
     if name == "c3":
         return dg.config_c3(1, n_queries=300), dict(config="c3", seed=1, n_queries=300)
     raise SystemExit(f"unknown dataset {name}")
@@ -227,7 +237,7 @@ def main():
     if not args.name:
         ap.error("name the dataset (c3 or c4)")
     name = args.name
-    out_path = os.path.join(HERE, f"{name}.json")
+    out_path = os.path.join(HERE, f"{FIXTURE_FILE.get(name, name)}.json")
     wl, spec = workload(name)
     queries = wl.queries
     fx = dict(name=name, spec=spec, checksum=mg.checksum(wl.graph, wl.groups), cells=[],

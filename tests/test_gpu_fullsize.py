@@ -122,7 +122,7 @@ def _large_fixture(name):
         fx = json.load(f)
     sys.path.insert(0, here)
     import make_golden as mg
-    wl = dg.config_c4(1, n_queries=300) if name == "c4" else dg.config_c3(1, n_queries=300)
+    wl = {"c4": dg.config_c4, "c3": dg.config_c3, "c2_batch": dg.config_c2}[name](1, n_queries=300)
     assert mg.checksum(wl.graph, wl.groups) == fx["checksum"], f"{name}: generator no longer reproduces the fixture"
     cells = [c for c in fx["cells"] if c.get("costs") and all(x is not None for x in c["costs"])]
     if not cells:
@@ -130,10 +130,11 @@ def _large_fixture(name):
     return fx, wl, cells
 
 
-@pytest.mark.parametrize("name", ["c4", "c3"])
+@pytest.mark.parametrize("name", ["c4", "c3", "c2_batch"])
 def test_benchmark_size_costs_equal_the_reference_binaries(name):
-    """C4 (4M vertices, the headline workload) and C3 (1M vertices, k=7 with
-    D in {2..5}): every pinned query of every (k, D) cell equals the cost the
+    """C4 (4M vertices, the headline workload), C3 (1M vertices, k=7 with
+    D in {2..5}) and the whole 300-query C2 batch (170k vertices, k=5): every
+    pinned query of every (k, D) cell equals the cost the
     reference PrunedDP++ / D-PrunedDP++ printed (for C4's k=7 D-bounded cells,
     whose reference table does not fit in memory, the cost of the HOP_cpu
     restatement oracle.hop_lean), solved as one batch; the first query of each

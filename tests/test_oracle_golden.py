@@ -96,9 +96,9 @@ def test_c2_fixture_regenerates_and_pins_the_restatement(golden):
         assert oracle.prunedpp(g, gr, ids)[0] == w
 
 
-@pytest.mark.parametrize("name", ["c3", "c4"])
+@pytest.mark.parametrize("name", ["c3", "c4", "c2_batch"])
 def test_benchmark_size_fixtures_reproduce(name):
-    """The C3 / C4 fixtures (made by tests/golden/make_golden_large.py from the
+    """The C3 / C4 / C2-batch fixtures (made by tests/golden/make_golden_large.py from the
     reference binaries) still describe what the generator builds, and their
     queries are the workload's own queries at the recorded indices."""
     import json
@@ -110,7 +110,7 @@ def test_benchmark_size_fixtures_reproduce(name):
     import make_golden as mg
     with open(os.path.join(here, f"{name}.json")) as f:
         fx = json.load(f)
-    wl = dg.config_c4(1, n_queries=300) if name == "c4" else dg.config_c3(1, n_queries=300)
+    wl = {"c4": dg.config_c4, "c3": dg.config_c3, "c2_batch": dg.config_c2}[name](1, n_queries=300)
     assert mg.checksum(wl.graph, wl.groups) == fx["checksum"]
     pinned = 0
     for c in fx["cells"]:
@@ -127,4 +127,4 @@ def test_benchmark_size_fixtures_reproduce(name):
             assert ids.tolist() == q and D == c["D"] and len(q) == c["k"]
             assert cost == oracle.INF or 0 < cost < oracle.INF
             pinned += 1
-    assert pinned >= (130 if name == "c4" else 18)
+    assert pinned >= {"c4": 130, "c3": 18, "c2_batch": 300}[name]
