@@ -57,8 +57,8 @@ import oracle  # noqa: E402
 # cell, D = -1 for plain.  n is set by what the reference finishes in
 # reasonable time on a few cores; 0 marks a cell the reference cannot run.
 SUBSETS = {
-    "c4": {(3, -1): 52, (5, -1): 24, (7, -1): 24,
-           (3, 2): 10, (3, 3): 10, (3, 4): 10, (3, 5): 10,
+    "c4": {(3, -1): 52, (5, -1): 51, (7, -1): 32,
+           (3, 2): 10, (3, 3): 10, (3, 4): 12, (3, 5): 12,
            (5, 2): 6, (5, 3): 6, (5, 4): 6, (5, 5): 6,
            (7, 2): 0, (7, 3): 0, (7, 4): 0, (7, 5): 0},
     "c3": {(7, 2): 10, (7, 3): 10, (7, 4): 6, (7, 5): 6},
@@ -69,7 +69,7 @@ SUBSETS = {
 FIXTURE_FILE = {"c2": "c2_batch"}
 # Cells pinned by the restatement (--restatement): the first n queries of
 # each cell the reference cannot run.
-LEAN_SUBSETS = {"c4": {(7, 2): 6, (7, 3): 6, (7, 4): 6, (7, 5): 6}}
+LEAN_SUBSETS = {"c4": {(7, 2): 14, (7, 3): 11, (7, 4): 10, (7, 5): 13}}
 LEAN_PROGRAM = "oracle.hop_lean"
 PLAIN_PER_JOB = 4  # plain queries per process (amortises the graph load)
 
@@ -349,6 +349,7 @@ def main():
 
             jobs.append(dict(argv=argv, cwd=d, mem=mem_bytes(wl, k, D), done=done,
                              label=f"{name} k={k} D={D} queries {[todo[x] for x in range(a, b + 1)]}"))
+    jobs.sort(key=lambda j: -j["mem"])  # largest tables (the longest queries) first
     save()
     log(f"{len(jobs)} jobs, {args.procs} processes, {args.mem_gb} GB")
     run_jobs(jobs, args.procs, args.mem_gb * 1e9, log)
