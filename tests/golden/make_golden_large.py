@@ -57,7 +57,7 @@ import oracle  # noqa: E402
 # cell, D = -1 for plain.  n is set by what the reference finishes in
 # reasonable time on a few cores; 0 marks a cell the reference cannot run.
 SUBSETS = {
-    "c4": {(3, -1): 52, (5, -1): 51, (7, -1): 32,
+    "c4": {(3, -1): 52, (5, -1): 51, (7, -1): 24,
            (3, 2): 10, (3, 3): 10, (3, 4): 12, (3, 5): 12,
            (5, 2): 6, (5, 3): 6, (5, 4): 6, (5, 5): 6,
            (7, 2): 0, (7, 3): 0, (7, 4): 0, (7, 5): 0},
